@@ -1,0 +1,189 @@
+/* ymgpu.h -- C ABI of libymgpu, the B200 (sm_100a) lattice gauge engine.
+ *
+ * Drop-in boundary for the data-parallel path of QSOLKCB/YANG-MILLS: link
+ * sweeps, gauge observables and glueball measurements.  The reference exposes
+ * that path as module-level Rust functions over owned host lattices
+ * (`Su3Lattice4`, `Lattice4`) and a `&mut SplitMix64`; this ABI keeps the
+ * same operations, argument meanings and fail-closed error behaviour, with
+ * lattices held on the device:
+ *
+ *   - an opaque `ym_ensemble` owns the device links of one or more chains
+ *     (one chain = one reference lattice; many chains of uneven extents can
+ *     share one handle and are updated by the same kernel launches);
+ *   - host lattices cross the boundary in the reference's own memory order
+ *     (`Vec<Su3>`/`Vec<Su2>` with link index site*4+mu, lexicographic sites,
+ *     x3 fastest; SU(3) = 18 doubles row-major re/im, SU(2) = 4 doubles);
+ *   - every call returns an int32 `ym_status` (include/ym_status.h), results
+ *     come back through caller-owned out-pointers, nothing panics;
+ *   - calls on one handle are not thread-safe (the reference takes
+ *     `&mut lattice`); each handle owns one CUDA stream.
+ *
+ * Random numbers: the reference draws from one SplitMix64 stream in
+ * lexicographic link order.  A checkerboard engine cannot split that stream,
+ * so every link visit owns a counter-based SplitMix64 stream keyed by
+ * (chain seed, sweep index, link):  key = S(S(seed, sweep), 4*site+mu) with
+ * S(k, n) = mix64(k + (n+1)*0x9E3779B97F4A7C15), the reference's own
+ * generator evaluated at a given position.  The per-link update rule and its
+ * arithmetic are the reference's.  ym_su3_reference_sweeps additionally
+ * replays the reference's single-stream lexicographic order bit for bit.
+ */
+#ifndef YMGPU_H
+#define YMGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "ym_status.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct ym_ensemble ym_ensemble;
+
+/* The cudaError_t behind the calling thread's most recent YM_ERR_CUDA. */
+int32_t ym_last_cuda_error(void);
+
+enum { YM_GROUP_SU2 = 2, YM_GROUP_SU3 = 3 };
+
+/* Link storage precision.  F64 keeps all 18 reals of an SU(3) link;
+ * F32_TWO_ROW keeps the first two rows in binary32 (12 reals) and rebuilds
+ * the third as the conjugate cross product. */
+enum { YM_PREC_F64 = 0, YM_PREC_F32_TWO_ROW = 1 };
+
+/* SU(3) Metropolis generator choice.  ORDERED: the reference's eight hits per
+ * link, generators 1..8 in order (su3_ensemble.rs:361).  UNIFORM: eight hits,
+ * each generator drawn uniformly from bits 52..54 of the hit's angle word
+ * (bits the angle grid does not use). */
+enum { YM_GEN_ORDERED = 0, YM_GEN_UNIFORM = 1 };
+
+typedef struct {
+    int32_t group;                /* YM_GROUP_SU2 or YM_GROUP_SU3 */
+    int32_t precision;            /* YM_PREC_* */
+    int64_t n_chains;             /* >= 1 */
+    const int64_t *extents;       /* n_chains x 4, every extent >= 2 */
+    const double *beta;           /* n_chains couplings (may differ) */
+    const uint64_t *chain_seed;   /* n_chains stream seeds */
+    int32_t lift_reference_caps;  /* 0: reject lattices above the reference's
+                                     link caps (2^18 SU(3), 2^20 SU(2)) */
+    int32_t device;               /* CUDA device ordinal */
+} ym_ensemble_desc;
+
+/* ---- handle lifetime (Su3Lattice4::new_identity su3_lattice.rs:85,
+ *      Lattice4::new_identity lib.rs:242) ---- */
+int32_t ym_ensemble_create(const ym_ensemble_desc *desc, ym_ensemble **out);
+int32_t ym_ensemble_destroy(ym_ensemble *ens);
+int32_t ym_ensemble_info(const ym_ensemble *ens, int64_t *n_chains, int64_t *total_links,
+                         int32_t *group, int32_t *precision);
+/* Cold start: every link the identity (all chains). */
+int32_t ym_ensemble_set_identity(ym_ensemble *ens);
+/* Hot start (no reference counterpart: the reference always starts cold,
+ * su3_ensemble.rs:412): every SU(3) link Haar-random, drawn from a stream
+ * keyed by the chain seed and the link index. */
+int32_t ym_ensemble_hot_start(ym_ensemble *ens);
+/* Copy one chain's links from/to a host array in the reference layout.
+ * Blocking with respect to the host buffer. */
+int32_t ym_ensemble_upload(ym_ensemble *ens, int64_t chain, const double *host_links);
+int32_t ym_ensemble_download(ym_ensemble *ens, int64_t chain, double *host_links);
+/* Sweep counter: the index the next sweep uses in the stream key. */
+int32_t ym_ensemble_set_sweep_index(ym_ensemble *ens, uint64_t sweep);
+int32_t ym_ensemble_get_sweep_index(ym_ensemble *ens, uint64_t *sweep);
+int32_t ym_ensemble_synchronize(ym_ensemble *ens);
+/* The handle's CUDA stream (cudaStream_t), for callers that order their own
+ * work after the engine's. */
+int32_t ym_ensemble_stream(ym_ensemble *ens, void **stream);
+
+/* ---- SU(3) Metropolis (su3_ensemble.rs:342-391 metropolis_sweep) ----
+ * n_sweeps checkerboard sweeps of every chain: parity 0 then 1, direction
+ * 0..3, eight hits per link visit, accept iff u < exp(-max(dS,0)).  Every
+ * extent must be even (YM_ERR_NOT_CHECKERBOARDABLE).  proposal_angle is the
+ * paired-grid half width, validated as in the reference (1e-8 <= a <= 1);
+ * beta per chain must lie in [0, 12]. */
+int32_t ym_su3_metropolis_sweeps(ym_ensemble *ens, double proposal_angle, int32_t generator_mode,
+                                 int64_t n_sweeps);
+/* Accumulated proposals/accepts per chain since creation or reset
+ * (MetropolisAccounting su3_ensemble.rs:117-121). */
+int32_t ym_su3_accounting(ym_ensemble *ens, uint64_t *proposals, uint64_t *accepts);
+int32_t ym_reset_accounting(ym_ensemble *ens);
+
+/* The reference's own sweep, replayed on the device one thread per chain:
+ * lexicographic link order, one SplitMix64 stream per chain whose state is
+ * read from and written back to rng_state[n_chains], twelve-plaquette action
+ * difference (su3_ensemble.rs:261-391).  Slow by design; it exists so the
+ * device reproduces the reference's chains exactly. */
+int32_t ym_su3_reference_sweeps(ym_ensemble *ens, double proposal_angle, uint64_t *rng_state,
+                                int64_t n_sweeps, uint64_t *proposals, uint64_t *accepts);
+/* Lexicographic sequential plaquette sum, one thread per chain: the
+ * reference's summation order (su3_ensemble.rs:228-259), bit for bit. */
+int32_t ym_su3_reference_average_plaquette(ym_ensemble *ens, double *per_chain);
+
+/* ---- observables ----
+ * Average plaquette per chain (su3_ensemble.rs:228 / su2_ensemble.rs:348):
+ * mean over sites and mu<nu of (1/N) Re Tr P, FP64 tree reduction in a fixed
+ * order (deterministic; within 1e-15 relative of the sequential sum). */
+int32_t ym_average_plaquette(ym_ensemble *ens, double *per_chain);
+/* Largest unitarity and determinant residual per chain
+ * (Su3Lattice4::max_link_*_residual su3_lattice.rs:285-297). */
+int32_t ym_su3_max_residuals(ym_ensemble *ens, double *unitarity, double *determinant);
+
+/* ---- host-side FP64 analysis and stream helpers ---- */
+
+/* ChainDiagnostics (su2_ensemble.rs:161-170); the autocorrelation series is
+ * written to a caller array of max_lag+1 doubles. */
+typedef struct {
+    double mean;
+    double variance;
+    int64_t positive_window_lag;
+    double integrated_autocorrelation_time;
+    double effective_sample_size;
+    double standard_error;
+} ym_chain_diagnostics;
+
+/* EfficiencyReport (sampling_efficiency.rs:22-34). */
+typedef struct {
+    ym_chain_diagnostics diagnostics;
+    double reweighting_efficiency;
+    double weight_only_ess;
+    double combined_ess_proxy;
+    double total_cost;
+    double sampling_cost_per_effective_sample_proxy;
+    double total_cost_per_effective_sample_proxy;
+} ym_efficiency_report;
+
+/* derive_chain_seed (su2_ensemble.rs:52-55) and derive_su3_chain_seed
+ * (su3_ensemble.rs:189-192). */
+uint64_t ym_derive_chain_seed(uint64_t master_seed, uint64_t chain_id);
+uint64_t ym_derive_su3_chain_seed(uint64_t master_seed, uint64_t chain_id);
+/* Output n (0-based) of SplitMix64::new(seed) (su2_ensemble.rs:29-37). */
+uint64_t ym_splitmix64_at(uint64_t seed, uint64_t n);
+/* proposal_angle_from_u64 (su3_ensemble.rs:199-213). */
+int32_t ym_proposal_angle_from_u64(uint64_t raw, double proposal_angle, double *out);
+/* diagnostics (su2_ensemble.rs:375-463). */
+int32_t ym_diagnostics(const double *values, int64_t n, int64_t max_lag,
+                       ym_chain_diagnostics *out, double *autocorrelation);
+/* evaluate (sampling_efficiency.rs:57-135); log_weights may be NULL. */
+int32_t ym_sampling_efficiency(const double *values, int64_t n, const double *log_weights,
+                               int64_t max_lag, double setup, double thermalization,
+                               double sampling, ym_efficiency_report *out,
+                               double *autocorrelation);
+
+/* ---- kernel timing (no reference counterpart: the reference counts cost in
+ * proposals only) ----  While enabled, each launch of the listed kernels is
+ * bracketed by CUDA events on the handle's stream; ym_profile_read
+ * synchronises, returns the summed device time and launch count of one
+ * kernel since the last read, and resets it. */
+enum { YM_KERNEL_SU3_METROPOLIS = 0, YM_KERNEL_PLAQUETTE = 1, YM_KERNEL_SU2_HEATBATH = 2,
+       YM_KERNEL_SU2_OVERRELAX = 3, YM_KERNEL_STOUT = 4, YM_KERNEL_OPERATORS = 5,
+       YM_KERNEL_AUX = 6, YM_KERNEL_COUNT = 8 };
+int32_t ym_profile_enable(ym_ensemble *ens, int32_t on);
+int32_t ym_profile_read(ym_ensemble *ens, int32_t kernel, double *total_ms, int64_t *launches);
+
+/* Per-chain coupling and stream seed (the reference passes beta and the
+ * stream to every sweep call, su3_ensemble.rs:342-347). */
+int32_t ym_ensemble_set_chain(ym_ensemble *ens, int64_t chain, double beta, uint64_t chain_seed);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* YMGPU_H */

@@ -15,7 +15,7 @@
  * This file restates the engine's order with the reference's arithmetic so
  * the device result can be compared bit for bit.  The only difference in the
  * SU(3) update is the action change: the engine contracts the candidate with
- * the staple sum, dS = beta*((ReTr(U A) - ReTr(U' A))/3), where the reference
+ * the staple sum, dS = (beta/3)*(ReTr(U A) - ReTr(U' A)), where the reference
  * multiplies out twelve plaquettes; the two agree to ~1e-15 and the tests
  * check that against or_su3_local_action_difference.
  *
@@ -219,7 +219,7 @@ static void su3_visit(mat3 *u, const mat3 *a, double beta, double angle, uint64_
         or_su3_generator_rotation(g, theta, (double *)&r);
         cand = rotate_rows(g, &r, u);
         double new_tr = retr_product(&cand, a);
-        double ds = beta * ((old_tr - new_tr) / 3.0);
+        double ds = (beta / 3.0) * (old_tr - new_tr);
         double acc = exp(-fmax(ds, 0.0));
         double uu = (double)(w_acc >> 11) * (1.0 / 9007199254740992.0);
         *np += 1;

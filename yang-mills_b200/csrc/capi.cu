@@ -1,0 +1,455 @@
+// capi.cu -- the extern "C" boundary of libymgpu (declared in include/ymgpu.h).
+//
+// Host-side mirror of the reference crate's lattice/ensemble entry points:
+// validation follows the reference's fail-closed checks in the same order
+// and reports the same variants (include/ym_status.h); device work is
+// enqueued on the handle's stream and synchronised before results return.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "ym_internal.hpp"
+
+using ym::ChainInfo;
+using ym::Tile;
+
+namespace {
+
+thread_local int g_last_cuda_error = 0;
+
+int32_t cuda_status(cudaError_t err) {
+    if (err == cudaSuccess) return YM_OK;
+    g_last_cuda_error = (int)err;
+    return YM_ERR_CUDA;
+}
+
+#define YM_CUDA(call)                                 \
+    do {                                              \
+        cudaError_t err__ = (call);                   \
+        if (err__ != cudaSuccess) return cuda_status(err__); \
+    } while (0)
+
+constexpr int64_t kMaxSu3Links = int64_t(1) << 18;   // su3_lattice.rs:17
+constexpr int64_t kMaxSu2Links = int64_t(1) << 20;   // lib.rs:21
+constexpr double kMaxSu3Beta = 12.0;                 // su3_ensemble.rs:24
+constexpr double kMinAngle = 1.0e-8;                 // su3_ensemble.rs:27
+constexpr double kMaxAngle = 1.0;                    // su3_ensemble.rs:28
+
+template <class T>
+cudaError_t dalloc(T **p, size_t count) {
+    return cudaMalloc(reinterpret_cast<void **>(p), count * sizeof(T) + 16);
+}
+
+void free_all(ym_ensemble *e) {
+    for (auto &pool : e->events)
+        for (auto &p : pool) {
+            cudaEventDestroy(p.start);
+            cudaEventDestroy(p.stop);
+        }
+    void *ptrs[] = {e->d_chains, e->d_half_tiles, e->d_site_tiles, e->d_site_tile_first,
+                    e->d_links, e->d_staging, e->d_partial, e->d_partial2, e->d_result,
+                    e->d_result2, e->d_accepts, e->d_sweep, e->d_rng, e->d_ref_counts};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    if (e->stream) cudaStreamDestroy(e->stream);
+}
+
+int32_t validate_angle(double a) {
+    if (!std::isfinite(a) || a < kMinAngle || a > kMaxAngle)
+        return YM_ERR_PROPOSAL_ANGLE_OUTSIDE_REFERENCE_RANGE;
+    return YM_OK;
+}
+
+int32_t validate_su3_betas(const ym_ensemble *e) {
+    for (const ChainInfo &c : e->chains)
+        if (!std::isfinite(c.beta) || c.beta < 0.0 || c.beta > kMaxSu3Beta)
+            return YM_ERR_BETA_OUTSIDE_REFERENCE_RANGE;
+    return YM_OK;
+}
+
+int32_t require_checkerboard(const ym_ensemble *e) {
+    for (const ChainInfo &c : e->chains)
+        for (int d = 0; d < 4; ++d)
+            if (c.n[d] % 2) return YM_ERR_NOT_CHECKERBOARDABLE;
+    return YM_OK;
+}
+
+int32_t set_device(const ym_ensemble *e) { return cuda_status(cudaSetDevice(e->device)); }
+
+// Runs `launch` and, when profiling is on, brackets it with an event pair.
+template <class F>
+cudaError_t timed(ym_ensemble *e, int kernel, F launch) {
+    if (!e->profiling) return launch();
+    auto &pool = e->events[kernel];
+    size_t &used = e->events_used[kernel];
+    if (used == pool.size()) {
+        ym_ensemble::EventPair p{};
+        cudaError_t err = cudaEventCreate(&p.start);
+        if (err == cudaSuccess) err = cudaEventCreate(&p.stop);
+        if (err != cudaSuccess) return err;
+        pool.push_back(p);
+    }
+    const ym_ensemble::EventPair &p = pool[used++];
+    cudaError_t err = cudaEventRecord(p.start, e->stream);
+    if (err == cudaSuccess) err = launch();
+    if (err == cudaSuccess) err = cudaEventRecord(p.stop, e->stream);
+    return err;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t ym_last_cuda_error(void) { return g_last_cuda_error; }
+
+int32_t ym_ensemble_create(const ym_ensemble_desc *desc, ym_ensemble **out) {
+    if (!desc || !out || !desc->extents || !desc->beta || !desc->chain_seed) return YM_ERR_NULL_ARGUMENT;
+    *out = nullptr;
+    if (desc->n_chains < 1 || desc->n_chains > (int64_t(1) << 30)) return YM_ERR_INVALID_ARGUMENT;
+    if (desc->group != YM_GROUP_SU3) return YM_ERR_WRONG_GROUP;
+    if (desc->precision != YM_PREC_F64) return YM_ERR_UNSUPPORTED_PRECISION;
+
+    ym_ensemble *e = new (std::nothrow) ym_ensemble();
+    if (!e) return YM_ERR_ALLOCATION_FAILED;
+    e->group = desc->group;
+    e->precision = desc->precision;
+    e->device = desc->device;
+    e->n_chains = desc->n_chains;
+    const int64_t per_link = (e->group == YM_GROUP_SU3) ? 9 : 2;   // double2 per link
+
+    // Lattice4::new_identity / Su3Lattice4::new_identity checks
+    // (lib.rs:242-263, su3_lattice.rs:85-106), per chain.
+    int64_t offset = 0;
+    for (int64_t ch = 0; ch < e->n_chains; ++ch) {
+        const int64_t *n = desc->extents + 4 * ch;
+        ChainInfo c{};
+        int64_t sites = 1;
+        for (int d = 0; d < 4; ++d) {
+            if (n[d] < 2) { delete e; return YM_ERR_INVALID_LATTICE_EXTENT; }
+        }
+        for (int d = 0; d < 4; ++d) {
+            if (n[d] > (int64_t(1) << 30) || sites > INT64_MAX / n[d]) { delete e; return YM_ERR_LATTICE_SIZE_OVERFLOW; }
+            sites *= n[d];
+            c.n[d] = (int32_t)n[d];
+        }
+        if (sites > INT64_MAX / 4) { delete e; return YM_ERR_LATTICE_SIZE_OVERFLOW; }
+        const int64_t links = sites * 4;
+        const int64_t cap = e->group == YM_GROUP_SU3 ? kMaxSu3Links : kMaxSu2Links;
+        if (!desc->lift_reference_caps && links > cap) { delete e; return YM_ERR_LATTICE_TOO_LARGE; }
+        c.eo = (n[3] % 2 == 0) ? 1 : 0;
+        c.volume = sites;
+        c.half = c.eo ? sites / 2 : sites;
+        c.offset = offset;
+        c.beta = desc->beta[ch];
+        c.seed = desc->chain_seed[ch];
+        offset += 4 * per_link * sites;
+        e->chains.push_back(c);
+        e->chain_links.push_back(links);
+        e->total_links += links;
+        if (links > e->max_chain_links) e->max_chain_links = links;
+    }
+    e->total_elems = offset;
+    e->proposals.assign((size_t)e->n_chains, 0);
+
+    // Work tiles: sub-sweeps cover the checkerboard half of every chain,
+    // measurements cover every site; a tile never straddles two chains.
+    std::vector<Tile> half, site;
+    std::vector<int32_t> first;
+    for (int64_t ch = 0; ch < e->n_chains; ++ch) {
+        const ChainInfo &c = e->chains[ch];
+        for (int64_t s = 0; s < c.half; s += ym::kSweepThreads) half.push_back(Tile{(int32_t)ch, 0, s});
+        first.push_back((int32_t)site.size());
+        for (int64_t s = 0; s < c.volume; s += ym::kSiteThreads) site.push_back(Tile{(int32_t)ch, 0, s});
+    }
+    first.push_back((int32_t)site.size());
+    e->n_half_tiles = (int64_t)half.size();
+    e->n_site_tiles = (int64_t)site.size();
+
+    cudaError_t err = cudaSetDevice(e->device);
+    if (err == cudaSuccess) err = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
+    if (err == cudaSuccess) err = dalloc(&e->d_chains, e->chains.size());
+    if (err == cudaSuccess) err = dalloc(&e->d_half_tiles, half.size());
+    if (err == cudaSuccess) err = dalloc(&e->d_site_tiles, site.size());
+    if (err == cudaSuccess) err = dalloc(&e->d_site_tile_first, first.size());
+    if (err == cudaSuccess) err = dalloc(&e->d_links, (size_t)e->total_elems);
+    if (err == cudaSuccess) err = dalloc(&e->d_staging, (size_t)e->max_chain_links * 18);
+    if (err == cudaSuccess) err = dalloc(&e->d_partial, site.size());
+    if (err == cudaSuccess) err = dalloc(&e->d_partial2, site.size());
+    if (err == cudaSuccess) err = dalloc(&e->d_result, (size_t)e->n_chains);
+    if (err == cudaSuccess) err = dalloc(&e->d_result2, (size_t)e->n_chains);
+    if (err == cudaSuccess) err = dalloc(&e->d_accepts, (size_t)e->n_chains);
+    if (err == cudaSuccess) err = dalloc(&e->d_sweep, 1);
+    if (err == cudaSuccess) err = dalloc(&e->d_rng, (size_t)e->n_chains);
+    if (err == cudaSuccess) err = dalloc(&e->d_ref_counts, 2 * (size_t)e->n_chains);
+    if (err == cudaSuccess)
+        err = cudaMemcpy(e->d_chains, e->chains.data(), e->chains.size() * sizeof(ChainInfo), cudaMemcpyHostToDevice);
+    if (err == cudaSuccess && !half.empty())
+        err = cudaMemcpy(e->d_half_tiles, half.data(), half.size() * sizeof(Tile), cudaMemcpyHostToDevice);
+    if (err == cudaSuccess && !site.empty())
+        err = cudaMemcpy(e->d_site_tiles, site.data(), site.size() * sizeof(Tile), cudaMemcpyHostToDevice);
+    if (err == cudaSuccess)
+        err = cudaMemcpy(e->d_site_tile_first, first.data(), first.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
+    if (err == cudaSuccess) err = cudaMemset(e->d_accepts, 0, (size_t)e->n_chains * sizeof(unsigned long long));
+    if (err == cudaSuccess) err = cudaMemset(e->d_sweep, 0, sizeof(uint64_t));
+    if (err == cudaSuccess) err = ym::launch_su3_identity(e);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);
+    if (err != cudaSuccess) {
+        free_all(e);
+        delete e;
+        if (err == cudaErrorMemoryAllocation) return YM_ERR_ALLOCATION_FAILED;
+        return cuda_status(err);
+    }
+    *out = e;
+    return YM_OK;
+}
+
+int32_t ym_ensemble_destroy(ym_ensemble *e) {
+    if (!e) return YM_ERR_NULL_ARGUMENT;
+    cudaSetDevice(e->device);
+    if (e->stream) cudaStreamSynchronize(e->stream);
+    free_all(e);
+    delete e;
+    return YM_OK;
+}
+
+int32_t ym_ensemble_info(const ym_ensemble *e, int64_t *n_chains, int64_t *total_links,
+                         int32_t *group, int32_t *precision) {
+    if (!e) return YM_ERR_NULL_ARGUMENT;
+    if (n_chains) *n_chains = e->n_chains;
+    if (total_links) *total_links = e->total_links;
+    if (group) *group = e->group;
+    if (precision) *precision = e->precision;
+    return YM_OK;
+}
+
+int32_t ym_ensemble_set_identity(ym_ensemble *e) {
+    if (!e) return YM_ERR_NULL_ARGUMENT;
+    int32_t st = set_device(e);
+    if (st) return st;
+    YM_CUDA(ym::launch_su3_identity(e));
+    YM_CUDA(cudaStreamSynchronize(e->stream));
+    return YM_OK;
+}
+
+int32_t ym_ensemble_hot_start(ym_ensemble *e) {
+    if (!e) return YM_ERR_NULL_ARGUMENT;
+    if (e->group != YM_GROUP_SU3) return YM_ERR_WRONG_GROUP;
+    int32_t st = set_device(e);
+    if (st) return st;
+    YM_CUDA(ym::launch_su3_hot_start(e));
+    YM_CUDA(cudaStreamSynchronize(e->stream));
+    return YM_OK;
+}
+
+int32_t ym_ensemble_upload(ym_ensemble *e, int64_t chain, const double *host) {
+    if (!e || !host) return YM_ERR_NULL_ARGUMENT;
+    if (chain < 0 || chain >= e->n_chains) return YM_ERR_INVALID_ARGUMENT;
+    int32_t st = set_device(e);
+    if (st) return st;
+    const size_t bytes = (size_t)e->chain_links[chain] * 18 * sizeof(double);
+    YM_CUDA(cudaMemcpyAsync(e->d_staging, host, bytes, cudaMemcpyHostToDevice, e->stream));
+    YM_CUDA(ym::launch_su3_from_aos(e, chain));
+    YM_CUDA(cudaStreamSynchronize(e->stream));
+    return YM_OK;
+}
+
+int32_t ym_ensemble_download(ym_ensemble *e, int64_t chain, double *host) {
+    if (!e || !host) return YM_ERR_NULL_ARGUMENT;
+    if (chain < 0 || chain >= e->n_chains) return YM_ERR_INVALID_ARGUMENT;
+    int32_t st = set_device(e);
+    if (st) return st;
+    const size_t bytes = (size_t)e->chain_links[chain] * 18 * sizeof(double);
+    YM_CUDA(ym::launch_su3_to_aos(e, chain));
+    YM_CUDA(cudaMemcpyAsync(host, e->d_staging, bytes, cudaMemcpyDeviceToHost, e->stream));
+    YM_CUDA(cudaStreamSynchronize(e->stream));
+    return YM_OK;
+}
+
+int32_t ym_ensemble_set_sweep_index(ym_ensemble *e, uint64_t sweep) {
+    if (!e) return YM_ERR_NULL_ARGUMENT;
+    int32_t st = set_device(e);
+    if (st) return st;
+    YM_CUDA(cudaMemcpyAsync(e->d_sweep, &sweep, sizeof sweep, cudaMemcpyHostToDevice, e->stream));
+    YM_CUDA(cudaStreamSynchronize(e->stream));
+    return YM_OK;
+}
+
+int32_t ym_ensemble_get_sweep_index(ym_ensemble *e, uint64_t *sweep) {
+    if (!e || !sweep) return YM_ERR_NULL_ARGUMENT;
+    int32_t st = set_device(e);
+    if (st) return st;
+    YM_CUDA(cudaMemcpyAsync(sweep, e->d_sweep, sizeof *sweep, cudaMemcpyDeviceToHost, e->stream));
+    YM_CUDA(cudaStreamSynchronize(e->stream));
+    return YM_OK;
+}
+
+int32_t ym_ensemble_set_chain(ym_ensemble *e, int64_t chain, double beta, uint64_t chain_seed) {
+    if (!e) return YM_ERR_NULL_ARGUMENT;
+    if (chain < 0 || chain >= e->n_chains) return YM_ERR_INVALID_ARGUMENT;
+    int32_t st = set_device(e);
+    if (st) return st;
+    e->chains[chain].beta = beta;
+    e->chains[chain].seed = chain_seed;
+    YM_CUDA(cudaMemcpyAsync(e->d_chains + chain, &e->chains[chain], sizeof(ChainInfo),
+                            cudaMemcpyHostToDevice, e->stream));
+    YM_CUDA(cudaStreamSynchronize(e->stream));
+    return YM_OK;
+}
+
+int32_t ym_ensemble_synchronize(ym_ensemble *e) {
+    if (!e) return YM_ERR_NULL_ARGUMENT;
+    int32_t st = set_device(e);
+    if (st) return st;
+    YM_CUDA(cudaStreamSynchronize(e->stream));
+    return YM_OK;
+}
+
+int32_t ym_ensemble_stream(ym_ensemble *e, void **stream) {
+    if (!e || !stream) return YM_ERR_NULL_ARGUMENT;
+    *stream = (void *)e->stream;
+    return YM_OK;
+}
+
+int32_t ym_su3_metropolis_sweeps(ym_ensemble *e, double angle, int32_t generator_mode,
+                                 int64_t n_sweeps) {
+    if (!e) return YM_ERR_NULL_ARGUMENT;
+    if (e->group != YM_GROUP_SU3) return YM_ERR_WRONG_GROUP;
+    // metropolis_sweep validates beta before the angle (su3_ensemble.rs:348-351)
+    int32_t st = validate_su3_betas(e);
+    if (st) return st;
+    st = validate_angle(angle);
+    if (st) return st;
+    if (generator_mode != YM_GEN_ORDERED && generator_mode != YM_GEN_UNIFORM) return YM_ERR_INVALID_ARGUMENT;
+    if (n_sweeps < 0) return YM_ERR_INVALID_ARGUMENT;
+    st = require_checkerboard(e);
+    if (st) return st;
+    st = set_device(e);
+    if (st) return st;
+    for (int64_t sw = 0; sw < n_sweeps; ++sw) {
+        for (int parity = 0; parity < 2; ++parity)
+            for (int mu = 0; mu < 4; ++mu)
+                YM_CUDA(timed(e, YM_KERNEL_SU3_METROPOLIS, [&] {
+                    return ym::launch_su3_metropolis(e, parity, mu, angle, generator_mode);
+                }));
+        YM_CUDA(ym::launch_advance_sweep(e));
+    }
+    for (int64_t ch = 0; ch < e->n_chains; ++ch)
+        e->proposals[ch] += (uint64_t)n_sweeps * 32u * (uint64_t)e->chains[ch].volume;
+    return YM_OK;
+}
+
+int32_t ym_su3_accounting(ym_ensemble *e, uint64_t *proposals, uint64_t *accepts) {
+    if (!e || !proposals || !accepts) return YM_ERR_NULL_ARGUMENT;
+    int32_t st = set_device(e);
+    if (st) return st;
+    YM_CUDA(cudaMemcpyAsync(accepts, e->d_accepts, (size_t)e->n_chains * sizeof(uint64_t),
+                            cudaMemcpyDeviceToHost, e->stream));
+    YM_CUDA(cudaStreamSynchronize(e->stream));
+    for (int64_t ch = 0; ch < e->n_chains; ++ch) proposals[ch] = e->proposals[ch];
+    return YM_OK;
+}
+
+int32_t ym_reset_accounting(ym_ensemble *e) {
+    if (!e) return YM_ERR_NULL_ARGUMENT;
+    int32_t st = set_device(e);
+    if (st) return st;
+    YM_CUDA(cudaMemsetAsync(e->d_accepts, 0, (size_t)e->n_chains * sizeof(unsigned long long), e->stream));
+    YM_CUDA(cudaStreamSynchronize(e->stream));
+    for (auto &p : e->proposals) p = 0;
+    return YM_OK;
+}
+
+int32_t ym_su3_reference_sweeps(ym_ensemble *e, double angle, uint64_t *rng_state,
+                                int64_t n_sweeps, uint64_t *proposals, uint64_t *accepts) {
+    if (!e || !rng_state) return YM_ERR_NULL_ARGUMENT;
+    if (e->group != YM_GROUP_SU3) return YM_ERR_WRONG_GROUP;
+    int32_t st = validate_su3_betas(e);
+    if (st) return st;
+    st = validate_angle(angle);
+    if (st) return st;
+    if (n_sweeps < 0) return YM_ERR_INVALID_ARGUMENT;
+    st = set_device(e);
+    if (st) return st;
+    const size_t nb = (size_t)e->n_chains * sizeof(uint64_t);
+    YM_CUDA(cudaMemcpyAsync(e->d_rng, rng_state, nb, cudaMemcpyHostToDevice, e->stream));
+    YM_CUDA(ym::launch_su3_reference_sweeps(e, angle, n_sweeps));
+    YM_CUDA(cudaMemcpyAsync(rng_state, e->d_rng, nb, cudaMemcpyDeviceToHost, e->stream));
+    std::vector<unsigned long long> counts(2 * (size_t)e->n_chains);
+    YM_CUDA(cudaMemcpyAsync(counts.data(), e->d_ref_counts, 2 * nb, cudaMemcpyDeviceToHost, e->stream));
+    YM_CUDA(cudaStreamSynchronize(e->stream));
+    for (int64_t ch = 0; ch < e->n_chains; ++ch) {
+        if (proposals) proposals[ch] = counts[ch];
+        if (accepts) accepts[ch] = counts[e->n_chains + ch];
+    }
+    return YM_OK;
+}
+
+int32_t ym_su3_reference_average_plaquette(ym_ensemble *e, double *per_chain) {
+    if (!e || !per_chain) return YM_ERR_NULL_ARGUMENT;
+    int32_t st = set_device(e);
+    if (st) return st;
+    YM_CUDA(ym::launch_su3_reference_plaquette(e));
+    YM_CUDA(cudaMemcpyAsync(per_chain, e->d_result, (size_t)e->n_chains * sizeof(double),
+                            cudaMemcpyDeviceToHost, e->stream));
+    YM_CUDA(cudaStreamSynchronize(e->stream));
+    for (int64_t ch = 0; ch < e->n_chains; ++ch)
+        if (!std::isfinite(per_chain[ch])) return YM_ERR_NON_FINITE_STATISTIC;
+    return YM_OK;
+}
+
+int32_t ym_average_plaquette(ym_ensemble *e, double *per_chain) {
+    if (!e || !per_chain) return YM_ERR_NULL_ARGUMENT;
+    int32_t st = set_device(e);
+    if (st) return st;
+    YM_CUDA(timed(e, YM_KERNEL_PLAQUETTE, [&] { return ym::launch_su3_plaquette(e); }));
+    YM_CUDA(cudaMemcpyAsync(per_chain, e->d_result, (size_t)e->n_chains * sizeof(double),
+                            cudaMemcpyDeviceToHost, e->stream));
+    YM_CUDA(cudaStreamSynchronize(e->stream));
+    for (int64_t ch = 0; ch < e->n_chains; ++ch)
+        if (!std::isfinite(per_chain[ch])) return YM_ERR_NON_FINITE_STATISTIC;
+    return YM_OK;
+}
+
+int32_t ym_su3_max_residuals(ym_ensemble *e, double *unitarity, double *determinant) {
+    if (!e || !unitarity || !determinant) return YM_ERR_NULL_ARGUMENT;
+    int32_t st = set_device(e);
+    if (st) return st;
+    YM_CUDA(ym::launch_su3_residuals(e));
+    YM_CUDA(cudaMemcpyAsync(unitarity, e->d_result, (size_t)e->n_chains * sizeof(double),
+                            cudaMemcpyDeviceToHost, e->stream));
+    YM_CUDA(cudaMemcpyAsync(determinant, e->d_result2, (size_t)e->n_chains * sizeof(double),
+                            cudaMemcpyDeviceToHost, e->stream));
+    YM_CUDA(cudaStreamSynchronize(e->stream));
+    return YM_OK;
+}
+
+int32_t ym_profile_enable(ym_ensemble *e, int32_t on) {
+    if (!e) return YM_ERR_NULL_ARGUMENT;
+    e->profiling = on != 0;
+    for (size_t &u : e->events_used) u = 0;
+    return YM_OK;
+}
+
+int32_t ym_profile_read(ym_ensemble *e, int32_t kernel, double *total_ms, int64_t *launches) {
+    if (!e || !total_ms || !launches) return YM_ERR_NULL_ARGUMENT;
+    if (kernel < 0 || kernel >= YM_KERNEL_COUNT) return YM_ERR_INVALID_ARGUMENT;
+    int32_t st = set_device(e);
+    if (st) return st;
+    YM_CUDA(cudaStreamSynchronize(e->stream));
+    double ms = 0.0;
+    for (size_t i = 0; i < e->events_used[kernel]; ++i) {
+        float t = 0.0f;
+        YM_CUDA(cudaEventElapsedTime(&t, e->events[kernel][i].start, e->events[kernel][i].stop));
+        ms += t;
+    }
+    *total_ms = ms;
+    *launches = (int64_t)e->events_used[kernel];
+    e->events_used[kernel] = 0;
+    return YM_OK;
+}
+
+}  // extern "C"

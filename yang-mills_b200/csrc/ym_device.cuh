@@ -1,0 +1,290 @@
+// ym_device.cuh -- device-side building blocks of the engine: complex and
+// 3x3 link algebra in the reference's operation order, counter-based
+// SplitMix64 streams, and the ensemble's storage geometry.
+//
+// Arithmetic contract: translation units that include this header for the
+// bit-reproducible FP64 path are compiled with -fmad=false, so every a*b+c
+// below is two rounded operations exactly as in the reference crate
+// (reference/rust/src/su3.rs:27-230) and the CPU oracle.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace ym {
+
+// ---------------------------------------------------------------- complex
+
+struct cplx {
+    double re, im;
+};
+
+__device__ __forceinline__ cplx cmake(double r, double i) { return cplx{r, i}; }
+__device__ __forceinline__ cplx cadd(cplx a, cplx b) { return cplx{a.re + b.re, a.im + b.im}; }
+__device__ __forceinline__ cplx csub(cplx a, cplx b) { return cplx{a.re - b.re, a.im - b.im}; }
+// Complex64::mul (su3.rs:57-62): (a.re*b.re - a.im*b.im, a.re*b.im + a.im*b.re)
+__device__ __forceinline__ cplx cmul(cplx a, cplx b) {
+    return cplx{a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+}
+__device__ __forceinline__ cplx cconj(cplx a) { return cplx{a.re, -a.im}; }
+
+// A 3x3 complex matrix held in registers, row-major.
+struct m3 {
+    cplx e[3][3];
+};
+
+// Mat3::mul (su3.rs:147-159): each entry accumulated over k = 0,1,2.  The
+// reference starts from an exact zero; adding +0 to the first product only
+// changes the sign of an exactly-zero entry, never a value.
+__device__ __forceinline__ m3 mul(const m3 &a, const m3 &b) {
+    m3 o;
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            cplx v = cmul(a.e[r][0], b.e[0][c]);
+            v = cadd(v, cmul(a.e[r][1], b.e[1][c]));
+            v = cadd(v, cmul(a.e[r][2], b.e[2][c]));
+            o.e[r][c] = v;
+        }
+    return o;
+}
+
+// a * b^dagger with the dagger materialised as conjugated entries first,
+// exactly as Mat3::dagger followed by Mat3::mul.
+__device__ __forceinline__ m3 mul_adj(const m3 &a, const m3 &b) {
+    m3 o;
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            cplx v = cmul(a.e[r][0], cconj(b.e[c][0]));
+            v = cadd(v, cmul(a.e[r][1], cconj(b.e[c][1])));
+            v = cadd(v, cmul(a.e[r][2], cconj(b.e[c][2])));
+            o.e[r][c] = v;
+        }
+    return o;
+}
+
+// a^dagger * b
+__device__ __forceinline__ m3 adj_mul(const m3 &a, const m3 &b) {
+    m3 o;
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            cplx v = cmul(cconj(a.e[0][r]), b.e[0][c]);
+            v = cadd(v, cmul(cconj(a.e[1][r]), b.e[1][c]));
+            v = cadd(v, cmul(cconj(a.e[2][r]), b.e[2][c]));
+            o.e[r][c] = v;
+        }
+    return o;
+}
+
+// a^dagger * b^dagger
+__device__ __forceinline__ m3 adj_mul_adj(const m3 &a, const m3 &b) {
+    m3 o;
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            cplx v = cmul(cconj(a.e[0][r]), cconj(b.e[c][0]));
+            v = cadd(v, cmul(cconj(a.e[1][r]), cconj(b.e[c][1])));
+            v = cadd(v, cmul(cconj(a.e[2][r]), cconj(b.e[c][2])));
+            o.e[r][c] = v;
+        }
+    return o;
+}
+
+__device__ __forceinline__ m3 adj(const m3 &a) {
+    m3 o;
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) o.e[r][c] = cconj(a.e[c][r]);
+    return o;
+}
+
+__device__ __forceinline__ void add_into(m3 &acc, const m3 &b) {
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) acc.e[r][c] = cadd(acc.e[r][c], b.e[r][c]);
+}
+
+__device__ __forceinline__ m3 identity3() {
+    m3 o;
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) o.e[r][c] = cmake(r == c ? 1.0 : 0.0, 0.0);
+    return o;
+}
+
+// Re Tr(P * B^dagger) computed from the diagonal of the product only:
+// Mat3::trace (su3.rs:171-173) sums the diagonal as (d0 + d1) + d2.
+__device__ __forceinline__ double retrace_mul_adj(const m3 &p, const m3 &b) {
+    double d[3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        cplx v = cmul(p.e[r][0], cconj(b.e[r][0]));
+        v = cadd(v, cmul(p.e[r][1], cconj(b.e[r][1])));
+        v = cadd(v, cmul(p.e[r][2], cconj(b.e[r][2])));
+        d[r] = v.re;
+    }
+    return (d[0] + d[1]) + d[2];
+}
+
+// Row contribution to Re Tr(X A): (t_i0 + t_i1) + t_i2,
+// t_ik = X_ik.re*A_ki.re - X_ik.im*A_ki.im.
+__device__ __forceinline__ double retr_row(const cplx *xrow, const m3 &a, int i) {
+    double t0 = xrow[0].re * a.e[0][i].re - xrow[0].im * a.e[0][i].im;
+    double t1 = xrow[1].re * a.e[1][i].re - xrow[1].im * a.e[1][i].im;
+    double t2 = xrow[2].re * a.e[2][i].re - xrow[2].im * a.e[2][i].im;
+    return (t0 + t1) + t2;
+}
+
+// ---------------------------------------------------------------- RNG
+
+constexpr uint64_t kGolden = 0x9E3779B97F4A7C15ULL;
+
+// SplitMix64 finaliser (su2_ensemble.rs:46-50).
+__device__ __forceinline__ uint64_t mix64(uint64_t v) {
+    v = (v ^ (v >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    v = (v ^ (v >> 27)) * 0x94D049BB133111EBULL;
+    return v ^ (v >> 31);
+}
+// Output n (0-based) of SplitMix64::new(seed): O(1) at any position.
+__device__ __forceinline__ uint64_t splitmix_at(uint64_t seed, uint64_t n) {
+    return mix64(seed + (n + 1) * kGolden);
+}
+// unit_f64 (su2_ensemble.rs:40-43): high 53 bits times 2^-53.
+__device__ __forceinline__ double unit_from(uint64_t w) {
+    return (double)(w >> 11) * (1.0 / 9007199254740992.0);
+}
+// Stream key of one link visit.
+__device__ __forceinline__ uint64_t link_key(uint64_t chain_seed, uint64_t sweep, int64_t lex,
+                                             int mu) {
+    return splitmix_at(splitmix_at(chain_seed, sweep), (uint64_t)(4 * lex + mu));
+}
+// proposal_angle_from_u64 (su3_ensemble.rs:199-213) for a validated angle.
+__device__ __forceinline__ double grid_angle(uint64_t raw, double angle) {
+    uint64_t m = raw & ((1ULL << 52) - 1);
+    double magnitude = angle * (double)(2 * m + 1) * (1.0 / 9007199254740992.0);
+    double sign = (raw >> 63) == 0 ? -1.0 : 1.0;
+    return sign * magnitude;
+}
+
+// ---------------------------------------------------------------- geometry
+
+// One chain of an ensemble.  Sites are stored in checkerboard order when the
+// last extent is even (storage = parity*Vh + lex/2), lexicographically
+// otherwise.  Links are structure-of-arrays: plane (mu, entry) holds one
+// complex (double2) per site; SU(3) has 9 entries per link, SU(2) stores its
+// quaternion as 2 complex entries.
+struct ChainInfo {
+    int32_t n[4];
+    int32_t eo;          // checkerboard storage order
+    int32_t pad;
+    int64_t volume;      // sites
+    int64_t half;        // volume / 2 (eo) or volume
+    int64_t offset;      // first double2 of this chain's block
+    double beta;
+    uint64_t seed;
+};
+
+struct Tile {
+    int32_t chain;
+    int32_t pad;
+    int64_t start;       // first work item of the tile within its chain
+};
+
+__device__ __forceinline__ int64_t storage_index(const ChainInfo &c, int64_t lex, int par) {
+    return c.eo ? (int64_t)par * c.half + (lex >> 1) : lex;
+}
+
+struct Coord {
+    int32_t x[4];
+    int64_t lex;
+    int par;
+};
+
+// Decode the site that storage slot `s` (0 <= s < volume) holds.
+__device__ __forceinline__ Coord decode_storage(const ChainInfo &c, int64_t s) {
+    Coord k;
+    int64_t lex;
+    if (c.eo) {
+        int par = s >= c.half ? 1 : 0;
+        int64_t t = s - (int64_t)par * c.half;
+        int64_t two_t = 2 * t;
+        int64_t row = two_t / c.n[3];
+        int x3b = (int)(two_t - row * c.n[3]);
+        k.x[2] = (int)(row % c.n[2]);
+        int64_t r2 = row / c.n[2];
+        k.x[1] = (int)(r2 % c.n[1]);
+        k.x[0] = (int)(r2 / c.n[1]);
+        int b = (par + k.x[0] + k.x[1] + k.x[2]) & 1;
+        k.x[3] = x3b + b;
+        lex = two_t + b;
+        k.par = par;
+    } else {
+        lex = s;
+        k.x[3] = (int)(s % c.n[3]);
+        int64_t r = s / c.n[3];
+        k.x[2] = (int)(r % c.n[2]);
+        r /= c.n[2];
+        k.x[1] = (int)(r % c.n[1]);
+        k.x[0] = (int)(r / c.n[1]);
+        k.par = (k.x[0] + k.x[1] + k.x[2] + k.x[3]) & 1;
+    }
+    k.lex = lex;
+    return k;
+}
+
+__device__ __forceinline__ int64_t stride_of(const ChainInfo &c, int d) {
+    int64_t s = 1;
+    for (int i = 3; i > d; --i) s *= c.n[i];
+    return s;
+}
+
+// Lexicographic index of x shifted by +1 (dir>0) or -1 along d.
+__device__ __forceinline__ int64_t shift_lex(const ChainInfo &c, const int32_t *x, int64_t lex,
+                                             int d, int dir) {
+    int64_t st = stride_of(c, d);
+    if (dir > 0) return x[d] == c.n[d] - 1 ? lex - (int64_t)(c.n[d] - 1) * st : lex + st;
+    return x[d] == 0 ? lex + (int64_t)(c.n[d] - 1) * st : lex - st;
+}
+
+// SU(3) FP64 link access: plane (mu*9 + entry) of a chain's block.
+__device__ __forceinline__ m3 load_su3(const double2 *__restrict__ links, const ChainInfo &c,
+                                       int64_t s, int mu) {
+    const double2 *p = links + c.offset + (int64_t)(mu * 9) * c.volume + s;
+    m3 o;
+#pragma unroll
+    for (int e = 0; e < 9; ++e) {
+        double2 v = __ldg(p + (int64_t)e * c.volume);
+        o.e[e / 3][e % 3] = cmake(v.x, v.y);
+    }
+    return o;
+}
+
+__device__ __forceinline__ m3 load_su3_rw(const double2 *links, const ChainInfo &c, int64_t s,
+                                          int mu) {
+    const double2 *p = links + c.offset + (int64_t)(mu * 9) * c.volume + s;
+    m3 o;
+#pragma unroll
+    for (int e = 0; e < 9; ++e) {
+        double2 v = p[(int64_t)e * c.volume];
+        o.e[e / 3][e % 3] = cmake(v.x, v.y);
+    }
+    return o;
+}
+
+__device__ __forceinline__ void store_su3(double2 *links, const ChainInfo &c, int64_t s, int mu,
+                                          const m3 &u) {
+    double2 *p = links + c.offset + (int64_t)(mu * 9) * c.volume + s;
+#pragma unroll
+    for (int e = 0; e < 9; ++e) p[(int64_t)e * c.volume] = make_double2(u.e[e / 3][e % 3].re, u.e[e / 3][e % 3].im);
+}
+
+}  // namespace ym

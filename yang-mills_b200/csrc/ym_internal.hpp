@@ -1,0 +1,73 @@
+// ym_internal.hpp -- host-side state of an ensemble handle and the launcher
+// interface between the C ABI (capi.cu) and the kernel translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "../../include/ymgpu.h"
+#include "ym_device.cuh"
+
+namespace ym {
+
+constexpr int kSweepThreads = 128;   // threads per tile of a sub-sweep
+constexpr int kSiteThreads = 128;    // threads per tile of a measurement
+
+}  // namespace ym
+
+struct ym_ensemble {
+    int32_t group = 3;
+    int32_t precision = YM_PREC_F64;
+    int32_t device = 0;
+    int64_t n_chains = 0;
+    std::vector<ym::ChainInfo> chains;     // host copy
+    std::vector<int64_t> chain_links;      // links per chain
+    int64_t total_links = 0;
+    int64_t max_chain_links = 0;
+    int64_t total_elems = 0;               // double2 elements of link storage
+
+    ym::ChainInfo *d_chains = nullptr;
+    ym::Tile *d_half_tiles = nullptr;      // work items = checkerboard half
+    int64_t n_half_tiles = 0;
+    ym::Tile *d_site_tiles = nullptr;      // work items = all sites
+    int64_t n_site_tiles = 0;
+    int32_t *d_site_tile_first = nullptr;  // first site tile of each chain (+ end)
+
+    double2 *d_links = nullptr;
+    double *d_staging = nullptr;           // AoS image of one chain
+    double *d_partial = nullptr;           // one double per site tile
+    double *d_partial2 = nullptr;          // second partial per site tile
+    double *d_result = nullptr;            // n_chains results
+    double *d_result2 = nullptr;
+    unsigned long long *d_accepts = nullptr;
+    uint64_t *d_sweep = nullptr;           // next sweep index
+    uint64_t *d_rng = nullptr;             // reference-replay stream states
+    unsigned long long *d_ref_counts = nullptr;  // reference replay: proposals, accepts
+    std::vector<uint64_t> proposals;       // host-counted proposals per chain
+
+    cudaStream_t stream = nullptr;
+
+    // Optional per-kernel timing: event pairs bracket each launch.
+    bool profiling = false;
+    struct EventPair { cudaEvent_t start, stop; };
+    std::vector<EventPair> events[8];
+    size_t events_used[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+};
+
+namespace ym {
+
+// Launchers implemented in su3_f64.cu (return a cudaError_t).
+cudaError_t launch_su3_identity(ym_ensemble *e);
+cudaError_t launch_su3_from_aos(ym_ensemble *e, int64_t chain);
+cudaError_t launch_su3_to_aos(ym_ensemble *e, int64_t chain);
+cudaError_t launch_su3_metropolis(ym_ensemble *e, int parity, int mu, double angle, int uniform);
+cudaError_t launch_advance_sweep(ym_ensemble *e);
+cudaError_t launch_su3_plaquette(ym_ensemble *e);
+cudaError_t launch_su3_residuals(ym_ensemble *e);
+cudaError_t launch_su3_reference_sweeps(ym_ensemble *e, double angle, int64_t n_sweeps);
+cudaError_t launch_su3_reference_plaquette(ym_ensemble *e);
+cudaError_t launch_su3_hot_start(ym_ensemble *e);
+
+}  // namespace ym

@@ -1,0 +1,17 @@
+"""ymgpu -- host mirror of the reference's lattice gauge API over libymgpu.
+
+The reference (QSOLKCB/YANG-MILLS) exposes its hot path as Rust module
+functions (``su3_ensemble``, ``su2_ensemble``, ``su3_lattice``, ...).  This
+package keeps those module and function names and calls the B200 engine
+through its C ABI (``include/ymgpu.h``).  There is no CPU fallback: importing
+a compute entry point without the built ``libymgpu.so`` raises.
+"""
+from ._lib import LIB_PATH, lib
+from .ensemble import Ensemble, F32_TWO_ROW, F64, ORDERED, SU2, SU3, UNIFORM
+from .errors import YmError
+from . import su2_ensemble, su3_ensemble, su3_lattice
+from .su3_lattice import Su3Lattice4
+
+__all__ = ["Ensemble", "Su3Lattice4", "YmError", "lib", "LIB_PATH", "su2_ensemble",
+           "su3_ensemble", "su3_lattice", "SU2", "SU3", "F64", "F32_TWO_ROW", "ORDERED",
+           "UNIFORM"]

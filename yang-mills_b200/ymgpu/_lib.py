@@ -1,0 +1,102 @@
+"""Loader of ``libymgpu.so`` (the engine's CUDA kernels behind a C ABI).
+
+The library is built in-tree (``yang-mills_b200/lib/libymgpu.so``) by
+``yang-mills_b200/csrc/Makefile``.  There is no CPU fallback: if the library
+is missing or no CUDA device answers, every entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_PKG), "lib", "libymgpu.so")
+
+i32, i64, u64, f64 = C.c_int32, C.c_int64, C.c_uint64, C.c_double
+P = C.POINTER
+VP = C.c_void_p
+
+
+class EnsembleDesc(C.Structure):
+    _fields_ = [("group", i32), ("precision", i32), ("n_chains", i64), ("extents", P(i64)),
+                ("beta", P(f64)), ("chain_seed", P(u64)), ("lift_reference_caps", i32),
+                ("device", i32)]
+
+
+# name -> (argtypes); every function returns int32 ym_status
+SIGNATURES = {
+    "ym_last_cuda_error": [],
+    "ym_ensemble_create": [P(EnsembleDesc), P(VP)],
+    "ym_ensemble_destroy": [VP],
+    "ym_ensemble_info": [VP, P(i64), P(i64), P(i32), P(i32)],
+    "ym_ensemble_set_identity": [VP],
+    "ym_ensemble_hot_start": [VP],
+    "ym_ensemble_upload": [VP, i64, P(f64)],
+    "ym_ensemble_download": [VP, i64, P(f64)],
+    "ym_ensemble_set_sweep_index": [VP, u64],
+    "ym_ensemble_get_sweep_index": [VP, P(u64)],
+    "ym_ensemble_synchronize": [VP],
+    "ym_ensemble_stream": [VP, P(VP)],
+    "ym_su3_metropolis_sweeps": [VP, f64, i32, i64],
+    "ym_su3_accounting": [VP, P(u64), P(u64)],
+    "ym_reset_accounting": [VP],
+    "ym_su3_reference_sweeps": [VP, f64, P(u64), i64, P(u64), P(u64)],
+    "ym_su3_reference_average_plaquette": [VP, P(f64)],
+    "ym_average_plaquette": [VP, P(f64)],
+    "ym_su3_max_residuals": [VP, P(f64), P(f64)],
+    "ym_ensemble_set_chain": [VP, i64, f64, u64],
+    "ym_proposal_angle_from_u64": [u64, f64, P(f64)],
+    "ym_profile_enable": [VP, i32],
+    "ym_profile_read": [VP, i32, P(f64), P(i64)],
+}
+
+KERNEL_IDS = {"su3_metropolis": 0, "plaquette": 1, "su2_heatbath": 2, "su2_overrelax": 3,
+              "stout": 4, "operators": 5, "aux": 6}
+
+
+class ChainDiagnostics(C.Structure):
+    _fields_ = [("mean", f64), ("variance", f64), ("positive_window_lag", i64),
+                ("integrated_autocorrelation_time", f64), ("effective_sample_size", f64),
+                ("standard_error", f64)]
+
+
+class EfficiencyReport(C.Structure):
+    _fields_ = [("diagnostics", ChainDiagnostics), ("reweighting_efficiency", f64),
+                ("weight_only_ess", f64), ("combined_ess_proxy", f64), ("total_cost", f64),
+                ("sampling_cost_per_effective_sample_proxy", f64),
+                ("total_cost_per_effective_sample_proxy", f64)]
+
+
+SIGNATURES.update({
+    "ym_diagnostics": [P(f64), i64, i64, P(ChainDiagnostics), P(f64)],
+    "ym_sampling_efficiency": [P(f64), i64, P(f64), i64, f64, f64, f64, P(EfficiencyReport),
+                               P(f64)],
+})
+U64_FUNCTIONS = {
+    "ym_derive_chain_seed": [u64, u64],
+    "ym_derive_su3_chain_seed": [u64, u64],
+    "ym_splitmix64_at": [u64, u64],
+}
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load libymgpu.so once; raise loudly when it is absent."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"libymgpu.so not built at {LIB_PATH}; run `make -C yang-mills_b200/csrc` "
+                "(the engine has no CPU fallback)")
+        L = C.CDLL(LIB_PATH)
+        for name, argtypes in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.argtypes = argtypes
+            fn.restype = i32
+        for name, argtypes in U64_FUNCTIONS.items():
+            fn = getattr(L, name)
+            fn.argtypes = argtypes
+            fn.restype = u64
+        _lib = L
+    return _lib

@@ -1,0 +1,175 @@
+"""Device ensembles: one or more lattices (chains) held on a B200.
+
+``Ensemble`` wraps the opaque ``ym_ensemble`` handle of libymgpu.  A chain is
+one reference lattice (``Su3Lattice4`` / ``Lattice4``); many chains of uneven
+extents share one handle and are updated by the same kernel launches.  Host
+lattices cross the boundary as numpy arrays in the reference's memory order:
+SU(3) ``(links, 3, 3)`` complex128, link index ``site*4 + mu`` with
+lexicographic sites, x3 fastest.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Sequence
+
+import numpy as np
+
+from ._lib import EnsembleDesc, lib
+from .errors import check
+
+SU2, SU3 = 2, 3
+F64, F32_TWO_ROW = 0, 1
+ORDERED, UNIFORM = 0, 1
+_GEN = {"ordered": ORDERED, "uniform": UNIFORM, ORDERED: ORDERED, UNIFORM: UNIFORM}
+
+
+def _f64p(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _u64p(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_uint64))
+
+
+class Ensemble:
+    """A set of chains resident in device memory (see include/ymgpu.h)."""
+
+    def __init__(self, extents: Sequence[Sequence[int]], beta, seeds, group: int = SU3,
+                 precision: int = F64, lift_reference_caps: bool = False, device: int = 0):
+        ext = np.ascontiguousarray(np.asarray(extents, dtype=np.int64).reshape(-1, 4))
+        n = ext.shape[0]
+        betas = np.ascontiguousarray(np.broadcast_to(np.asarray(beta, np.float64), (n,)).copy())
+        sd = np.ascontiguousarray(np.broadcast_to(np.asarray(seeds, np.uint64), (n,)).copy())
+        desc = EnsembleDesc(group, precision, n, ext.ctypes.data_as(C.POINTER(C.c_int64)),
+                            _f64p(betas), _u64p(sd), int(lift_reference_caps), device)
+        h = C.c_void_p()
+        check(lib().ym_ensemble_create(C.byref(desc), C.byref(h)), "ym_ensemble_create")
+        self._h = h
+        self.extents = [tuple(int(v) for v in row) for row in ext]
+        self.beta = betas
+        self.seeds = sd
+        self.group = group
+        self.precision = precision
+        self.n_chains = n
+
+    # ------------------------------------------------------------ lifetime
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            check(lib().ym_ensemble_destroy(self._h), "ym_ensemble_destroy")
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    def links_in_chain(self, chain: int) -> int:
+        return int(np.prod(self.extents[chain])) * 4
+
+    # ------------------------------------------------------------ state
+    def set_identity(self) -> None:
+        check(lib().ym_ensemble_set_identity(self._h), "set_identity")
+
+    def hot_start(self) -> None:
+        check(lib().ym_ensemble_hot_start(self._h), "hot_start")
+
+    def upload(self, chain: int, links: np.ndarray) -> None:
+        a = np.ascontiguousarray(links, dtype=np.complex128)
+        if a.size != self.links_in_chain(chain) * 9:
+            raise ValueError("link array does not match the chain's extents")
+        check(lib().ym_ensemble_upload(self._h, chain, _f64p(a.view(np.float64))), "upload")
+
+    def download(self, chain: int, out: np.ndarray | None = None) -> np.ndarray:
+        if out is None:
+            out = np.empty((self.links_in_chain(chain), 3, 3), np.complex128)
+        check(lib().ym_ensemble_download(self._h, chain, _f64p(out.view(np.float64))), "download")
+        return out
+
+    def set_chain(self, chain: int, beta: float, seed: int) -> None:
+        check(lib().ym_ensemble_set_chain(self._h, chain, float(beta), int(seed)), "set_chain")
+        self.beta[chain] = beta
+        self.seeds[chain] = seed
+
+    @property
+    def sweep_index(self) -> int:
+        v = C.c_uint64()
+        check(lib().ym_ensemble_get_sweep_index(self._h, C.byref(v)), "get_sweep_index")
+        return v.value
+
+    @sweep_index.setter
+    def sweep_index(self, value: int) -> None:
+        check(lib().ym_ensemble_set_sweep_index(self._h, int(value)), "set_sweep_index")
+
+    def synchronize(self) -> None:
+        check(lib().ym_ensemble_synchronize(self._h), "synchronize")
+
+    def stream(self) -> int:
+        p = C.c_void_p()
+        check(lib().ym_ensemble_stream(self._h, C.byref(p)), "stream")
+        return p.value or 0
+
+    # ------------------------------------------------------------ SU(3) updates
+    def metropolis_sweeps(self, proposal_angle: float, n_sweeps: int = 1,
+                          generator_mode="ordered") -> None:
+        check(lib().ym_su3_metropolis_sweeps(self._h, float(proposal_angle), _GEN[generator_mode],
+                                             int(n_sweeps)), "su3_metropolis_sweeps")
+
+    def accounting(self):
+        p = np.zeros(self.n_chains, np.uint64)
+        a = np.zeros(self.n_chains, np.uint64)
+        check(lib().ym_su3_accounting(self._h, _u64p(p), _u64p(a)), "su3_accounting")
+        return p, a
+
+    def reset_accounting(self) -> None:
+        check(lib().ym_reset_accounting(self._h), "reset_accounting")
+
+    def reference_sweeps(self, proposal_angle: float, rng_state, n_sweeps: int = 1):
+        st = np.ascontiguousarray(np.broadcast_to(np.asarray(rng_state, np.uint64),
+                                                  (self.n_chains,)).copy())
+        p = np.zeros(self.n_chains, np.uint64)
+        a = np.zeros(self.n_chains, np.uint64)
+        check(lib().ym_su3_reference_sweeps(self._h, float(proposal_angle), _u64p(st),
+                                            int(n_sweeps), _u64p(p), _u64p(a)),
+              "su3_reference_sweeps")
+        return st, p, a
+
+    # ------------------------------------------------------------ timing
+    def profile(self, on: bool = True) -> None:
+        check(lib().ym_profile_enable(self._h, int(on)), "profile_enable")
+
+    def profile_read(self, kernel: str):
+        """(total device ms, launches) of one kernel since the last read."""
+        from ._lib import KERNEL_IDS
+        ms, n = C.c_double(), C.c_int64()
+        check(lib().ym_profile_read(self._h, KERNEL_IDS[kernel], C.byref(ms), C.byref(n)),
+              "profile_read")
+        return ms.value, n.value
+
+    # ------------------------------------------------------------ observables
+    def average_plaquette(self) -> np.ndarray:
+        out = np.zeros(self.n_chains, np.float64)
+        check(lib().ym_average_plaquette(self._h, _f64p(out)), "average_plaquette")
+        return out
+
+    def reference_average_plaquette(self) -> np.ndarray:
+        out = np.zeros(self.n_chains, np.float64)
+        check(lib().ym_su3_reference_average_plaquette(self._h, _f64p(out)),
+              "reference_average_plaquette")
+        return out
+
+    def max_residuals(self):
+        u = np.zeros(self.n_chains, np.float64)
+        d = np.zeros(self.n_chains, np.float64)
+        check(lib().ym_su3_max_residuals(self._h, _f64p(u), _f64p(d)), "su3_max_residuals")
+        return u, d
