@@ -141,9 +141,20 @@ int or_su3_generator_rotation(int g, double theta, double *out18) {
     return YM_OK;
 }
 
+/* acc += a*b as four fused multiply-adds in a fixed order (the engine's
+ * staple and trace formulation; C99 fma() rounds exactly like the device). */
+static inline void c_fma_acc(c64 *acc, c64 a, c64 b) {
+    acc->re = fma(a.re, b.re, acc->re);
+    acc->re = fma(-a.im, b.im, acc->re);
+    acc->im = fma(a.re, b.im, acc->im);
+    acc->im = fma(a.im, b.re, acc->im);
+}
+
 /* Staple sum A = sum_{nu != mu} [U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag
  *                              + U_nu(x-nu+mu)^dag U_mu(x-nu)^dag U_nu(x-nu)],
- * nu ascending, forward then backward, dense unchecked products. */
+ * nu ascending, forward then backward.  Each term: P = product of the first
+ * two factors as fma chains from zero (j = 0,1,2), then A[r][c] += P[r][k] *
+ * third[k][c] as fma chains over k = 0,1,2 into the running sum. */
 static mat3 su3_staple(const extents4 *e, const double *links, const int64_t x[4], int mu) {
     mat3 a = m3_zero();
     for (int nu = 0; nu < 4; ++nu) {
@@ -151,15 +162,31 @@ static mat3 su3_staple(const extents4 *e, const double *links, const int64_t x[4
         int64_t xpm[4], xpn[4], xmn[4], xmnpm[4];
         nb_plus(e, x, mu, xpm);
         nb_plus(e, x, nu, xpn);
-        mat3 f = m3_mul(m3_mul(su3_link(e, links, xpm, nu), m3_dagger(su3_link(e, links, xpn, mu))),
-                        m3_dagger(su3_link(e, links, x, nu)));
-        a = m3_add(a, f);
         nb_minus(e, x, nu, xmn);
         nb_plus(e, xmn, mu, xmnpm);
-        mat3 b = m3_mul(m3_mul(m3_dagger(su3_link(e, links, xmnpm, nu)),
-                               m3_dagger(su3_link(e, links, xmn, mu))),
-                        su3_link(e, links, xmn, nu));
-        a = m3_add(a, b);
+        mat3 l1 = su3_link(e, links, xpm, nu), l2 = su3_link(e, links, xpn, mu);
+        mat3 l3 = su3_link(e, links, x, nu), p;
+        for (int r = 0; r < 3; ++r)
+            for (int k = 0; k < 3; ++k) {
+                c64 v = c_make(0.0, 0.0);
+                for (int j = 0; j < 3; ++j) c_fma_acc(&v, l1.m[r][j], c_conj(l2.m[k][j]));
+                p.m[r][k] = v;
+            }
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c)
+                for (int k = 0; k < 3; ++k) c_fma_acc(&a.m[r][c], p.m[r][k], c_conj(l3.m[c][k]));
+        l1 = su3_link(e, links, xmnpm, nu);
+        l2 = su3_link(e, links, xmn, mu);
+        l3 = su3_link(e, links, xmn, nu);
+        for (int r = 0; r < 3; ++r)
+            for (int k = 0; k < 3; ++k) {
+                c64 v = c_make(0.0, 0.0);
+                for (int j = 0; j < 3; ++j) c_fma_acc(&v, c_conj(l1.m[j][r]), c_conj(l2.m[k][j]));
+                p.m[r][k] = v;
+            }
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c)
+                for (int k = 0; k < 3; ++k) c_fma_acc(&a.m[r][c], p.m[r][k], l3.m[k][c]);
     }
     return a;
 }
@@ -173,15 +200,20 @@ int or_su3_staple(const int64_t *ext, const double *links, const int64_t *x, int
     return YM_OK;
 }
 
-/* ReTr(X A) = (r0 + r1) + r2, r_i = (t_i0 + t_i1) + t_i2,
- * t_ik = X_ik.re A_ki.re - X_ik.im A_ki.im. */
+/* ReTr(X A) = (r0 + r1) + r2 with row i a fused chain:
+ * r = x0.re*a0.re; r = fma(-x0.im, a0.im, r); r = fma(x1.re, a1.re, r);
+ * r = fma(-x1.im, a1.im, r); r = fma(x2.re, a2.re, r); r = fma(-x2.im, a2.im, r)
+ * where a_k = A[k][i]. */
 static double retr_product(const mat3 *x, const mat3 *a) {
     double r[3];
     for (int i = 0; i < 3; ++i) {
-        double t0 = x->m[i][0].re * a->m[0][i].re - x->m[i][0].im * a->m[0][i].im;
-        double t1 = x->m[i][1].re * a->m[1][i].re - x->m[i][1].im * a->m[1][i].im;
-        double t2 = x->m[i][2].re * a->m[2][i].re - x->m[i][2].im * a->m[2][i].im;
-        r[i] = (t0 + t1) + t2;
+        double acc = x->m[i][0].re * a->m[0][i].re;
+        acc = fma(-x->m[i][0].im, a->m[0][i].im, acc);
+        acc = fma(x->m[i][1].re, a->m[1][i].re, acc);
+        acc = fma(-x->m[i][1].im, a->m[1][i].im, acc);
+        acc = fma(x->m[i][2].re, a->m[2][i].re, acc);
+        acc = fma(-x->m[i][2].im, a->m[2][i].im, acc);
+        r[i] = acc;
     }
     return (r[0] + r[1]) + r[2];
 }

@@ -1,274 +1,19 @@
-// su3_f64.cu -- SU(3) kernels of the FP64 path (compiled with -fmad=false).
+// su3_f64.cu -- SU(3) measurement, replay and layout kernels of the FP64
+// path (compiled with -fmad=false; the sweep itself is su3_metropolis.cu).
 //
-//   k_su3_metropolis      one checkerboard sub-sweep (parity, mu) of every
-//                         chain: staple sum -> eight Metropolis hits -> store
-//                         (su3_ensemble.rs:342-391, update rule per link)
 //   k_su3_plaquette       per-tile plaquette sums  (su3_ensemble.rs:228-259)
-//   k_chain_sum/max       fixed-order per-chain reductions of tile partials
+//   k_chain_reduce        fixed-order per-chain reductions of tile partials
 //   k_su3_residuals       unitarity / determinant residuals (su3_lattice.rs:285-297)
 //   k_su3_reference_*     the reference's lexicographic single-stream sweep and
 //                         sequential plaquette, one thread per chain
+//   k_su3_hot_start       Haar-random links
 //   k_su3_{identity,from_aos,to_aos}  layout conversion, reference <-> SoA
-//
-// Each link visit draws from its own counter-based SplitMix64 stream (see
-// ym_device.cuh); the proposal exponential is evaluated by the scalar Taylor
-// recurrence the reference's dense series reduces to for one generator, so
-// candidates are bitwise the reference's (su3.rs:409-450).
 #include <cuda_runtime.h>
 
+#include "su3_exp.cuh"
 #include "ym_internal.hpp"
 
 namespace ym {
-
-// fl(1/k) for k = 0..67: the factors Mat3::scale_real(1.0 / order) applies
-// (su3.rs:435); filled once from the host with IEEE division.
-__constant__ double c_inv[68];
-
-// ------------------------------------------------------------ exponential
-
-constexpr double kTermCutoff = 1.0e-18;   // EXP_TERM_CUTOFF su3.rs:25
-
-// Taylor recurrence of one generator: t_k = (t_{k-1} h) fl(1/k); the
-// rotation block is c = 1 - t2 + t4 ..., s = t1 - t3 + ....  Stops after the
-// first term with |t_k| <= 1e-18, at most 64 terms (su3.rs:434-440).
-__device__ __forceinline__ void taylor_chain(double h, double &c, double &s) {
-    double t = 1.0;
-    c = 1.0;
-    s = 0.0;
-#pragma unroll 1
-    for (int k = 1; k <= 64; k += 4) {
-        t = (t * h) * c_inv[k];
-        s = s + t;
-        if (fabs(t) <= kTermCutoff) return;
-        t = (t * h) * c_inv[k + 1];
-        c = c - t;
-        if (fabs(t) <= kTermCutoff) return;
-        t = (t * h) * c_inv[k + 2];
-        s = s - t;
-        if (fabs(t) <= kTermCutoff) return;
-        t = (t * h) * c_inv[k + 3];
-        c = c + t;
-        if (fabs(t) <= kTermCutoff) return;
-    }
-}
-
-// Two diagonal chains advanced together (generator 8): the series stops on
-// the larger term, as Mat3::max_abs_entry does.
-__device__ __forceinline__ void taylor_chain2(double h1, double h2, double &c1, double &s1,
-                                              double &c2, double &s2) {
-    double t1 = 1.0, t2 = 1.0;
-    c1 = 1.0; s1 = 0.0; c2 = 1.0; s2 = 0.0;
-#pragma unroll 1
-    for (int k = 1; k <= 64; k += 4) {
-        t1 = (t1 * h1) * c_inv[k];     t2 = (t2 * h2) * c_inv[k];
-        s1 = s1 + t1;                  s2 = s2 + t2;
-        if (fmax(fabs(t1), fabs(t2)) <= kTermCutoff) return;
-        t1 = (t1 * h1) * c_inv[k + 1]; t2 = (t2 * h2) * c_inv[k + 1];
-        c1 = c1 - t1;                  c2 = c2 - t2;
-        if (fmax(fabs(t1), fabs(t2)) <= kTermCutoff) return;
-        t1 = (t1 * h1) * c_inv[k + 2]; t2 = (t2 * h2) * c_inv[k + 2];
-        s1 = s1 - t1;                  s2 = s2 - t2;
-        if (fmax(fabs(t1), fabs(t2)) <= kTermCutoff) return;
-        t1 = (t1 * h1) * c_inv[k + 3]; t2 = (t2 * h2) * c_inv[k + 3];
-        c1 = c1 + t1;                  c2 = c2 + t2;
-        if (fmax(fabs(t1), fabs(t2)) <= kTermCutoff) return;
-    }
-}
-
-// The (scaled) coefficient entries of i*theta*T^a: h = fl(0.5*theta) for the
-// seven off-diagonal/sigma_3 generators; for T^8 the diagonal entries are
-// fl((0.5/sqrt3)*theta) twice and fl((-1/sqrt3)*theta) (su3.rs:325-352,395-407).
-constexpr double kInvSqrt3 = 0.5773502691896258;   // su3.rs:22
-
-// Generator 8 rotation: diag(e1, e1, e2) with at most one squaring for
-// |theta| <= 1 (1-norm |theta|/sqrt3 may exceed 0.5).
-__device__ __forceinline__ void lambda8_rotation(double theta, cplx &e1, cplx &e2) {
-    double d1 = (0.5 * kInvSqrt3) * theta;
-    double d2 = (-kInvSqrt3) * theta;
-    int sq = 0;
-    double nrm = fmax(fabs(d1), fabs(d2));
-    while (nrm > 0.5) {
-        sq++;
-        nrm *= 0.5;
-    }
-    double sc = ldexp(1.0, -sq);
-    double c1, s1, c2, s2;
-    taylor_chain2(d1 * sc, d2 * sc, c1, s1, c2, s2);
-    e1 = cmake(c1, s1);
-    e2 = cmake(c2, s2);
-    for (int k = 0; k < sq; ++k) {
-        e1 = cmul(e1, e1);
-        e2 = cmul(e2, e2);
-    }
-}
-
-// ------------------------------------------------------------ link visit
-
-// Eight Metropolis hits on link u with staple sum a.  rr[i] caches row i of
-// Re Tr(u a); old_tr = (rr0 + rr1) + rr2.  beta3 = beta / 3.
-// Candidate rows follow Mat3::mul of the rotation with u: the block rotation
-// [[r00, r01], [r10, r11]] enters in ascending index order; untouched rows are
-// bitwise unchanged.  Returns the number of accepted hits.
-template <int I0, int I1>
-__device__ __forceinline__ void try_block(m3 &u, const m3 &a, double rr[3], double &old_tr,
-                                          int kind, double c, double s, double beta3, double unif,
-                                          unsigned &accepted) {
-    cplx n0[3], n1[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        const double x0 = u.e[I0][k].re, y0 = u.e[I0][k].im;
-        const double x1 = u.e[I1][k].re, y1 = u.e[I1][k].im;
-        if (kind == 0) {          // i h sigma_1: [[c, i s], [i s, c]]
-            n0[k] = cmake(c * x0 - s * y1, c * y0 + s * x1);
-            n1[k] = cmake(c * x1 - s * y0, s * x0 + c * y1);
-        } else if (kind == 1) {   // i h sigma_2: [[c, s], [-s, c]]
-            n0[k] = cmake(c * x0 + s * x1, c * y0 + s * y1);
-            n1[k] = cmake(c * x1 - s * x0, c * y1 - s * y0);
-        } else {                  // i h sigma_3: diag(c + i s, c - i s)
-            n0[k] = cmake(c * x0 - s * y0, c * y0 + s * x0);
-            n1[k] = cmake(c * x1 + s * y1, c * y1 - s * x1);
-        }
-    }
-    double q[3] = {rr[0], rr[1], rr[2]};
-    q[I0] = retr_row(n0, a, I0);
-    q[I1] = retr_row(n1, a, I1);
-    const double new_tr = (q[0] + q[1]) + q[2];
-    const double ds = beta3 * (old_tr - new_tr);
-    const double m = fmax(ds, 0.0);
-    const bool accept = (m == 0.0) ? true : (unif < exp(-m));
-    if (accept) {
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            u.e[I0][k] = n0[k];
-            u.e[I1][k] = n1[k];
-        }
-        rr[I0] = q[I0];
-        rr[I1] = q[I1];
-        old_tr = new_tr;
-        accepted++;
-    }
-}
-
-__device__ __forceinline__ void try_diag(m3 &u, const m3 &a, double rr[3], double &old_tr,
-                                         cplx e1, cplx e2, double beta3, double unif,
-                                         unsigned &accepted) {
-    cplx n[3][3];
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-        const cplx e = i < 2 ? e1 : e2;
-#pragma unroll
-        for (int k = 0; k < 3; ++k) n[i][k] = cmul(e, u.e[i][k]);
-    }
-    double q[3];
-#pragma unroll
-    for (int i = 0; i < 3; ++i) q[i] = retr_row(n[i], a, i);
-    const double new_tr = (q[0] + q[1]) + q[2];
-    const double ds = beta3 * (old_tr - new_tr);
-    const double m = fmax(ds, 0.0);
-    const bool accept = (m == 0.0) ? true : (unif < exp(-m));
-    if (accept) {
-#pragma unroll
-        for (int i = 0; i < 3; ++i) {
-#pragma unroll
-            for (int k = 0; k < 3; ++k) u.e[i][k] = n[i][k];
-            rr[i] = q[i];
-        }
-        old_tr = new_tr;
-        accepted++;
-    }
-}
-
-__device__ __forceinline__ unsigned visit_link(m3 &u, const m3 &a, double beta3, double angle,
-                                               uint64_t key, int uniform) {
-    double rr[3];
-#pragma unroll
-    for (int i = 0; i < 3; ++i) rr[i] = retr_row(u.e[i], a, i);
-    double old_tr = (rr[0] + rr[1]) + rr[2];
-    unsigned accepted = 0;
-#pragma unroll 1
-    for (int h = 0; h < 8; ++h) {
-        const uint64_t w_angle = splitmix_at(key, (uint64_t)(2 * h));
-        const uint64_t w_acc = splitmix_at(key, (uint64_t)(2 * h + 1));
-        const int g = uniform ? (int)((w_angle >> 52) & 7) : h;
-        const double theta = grid_angle(w_angle, angle);
-        const double unif = unit_from(w_acc);
-        if (g == 7) {
-            cplx e1, e2;
-            lambda8_rotation(theta, e1, e2);
-            try_diag(u, a, rr, old_tr, e1, e2, beta3, unif, accepted);
-        } else {
-            double c, s;
-            taylor_chain(0.5 * theta, c, s);   // |0.5 theta| < 0.5: no squaring
-            const int kind = (g == 2) ? 2 : ((g == 1 || g == 4 || g == 6) ? 1 : 0);
-            if (g <= 2)
-                try_block<0, 1>(u, a, rr, old_tr, kind, c, s, beta3, unif, accepted);
-            else if (g <= 4)
-                try_block<0, 2>(u, a, rr, old_tr, kind, c, s, beta3, unif, accepted);
-            else
-                try_block<1, 2>(u, a, rr, old_tr, kind, c, s, beta3, unif, accepted);
-        }
-    }
-    return accepted;
-}
-
-// Staple sum of link (x, mu): sum over nu != mu (ascending) of
-//   U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag  +  U_nu(x-nu+mu)^dag U_mu(x-nu)^dag U_nu(x-nu),
-// the SU(3) form of Lattice4::staple (lib.rs:507-546).  x has parity par.
-__device__ __forceinline__ m3 staple_sum(const double2 *__restrict__ links, const ChainInfo &c,
-                                         const Coord &x, int par, int mu) {
-    m3 acc;
-    bool first = true;
-    const int opp = par ^ 1;
-    const int64_t lex_pm = shift_lex(c, x.x, x.lex, mu, +1);
-#pragma unroll 1
-    for (int nu = 0; nu < 4; ++nu) {
-        if (nu == mu) continue;
-        const int64_t lex_pn = shift_lex(c, x.x, x.lex, nu, +1);
-        const int64_t lex_mn = shift_lex(c, x.x, x.lex, nu, -1);
-        const int64_t lex_mnpm = shift_lex(c, x.x, lex_mn, mu, +1);
-        {
-            m3 p = mul_adj(load_su3(links, c, storage_index(c, lex_pm, opp), nu),
-                           load_su3(links, c, storage_index(c, lex_pn, opp), mu));
-            m3 f = mul_adj(p, load_su3(links, c, storage_index(c, x.lex, par), nu));
-            if (first) {
-                acc = f;
-                first = false;
-            } else {
-                add_into(acc, f);
-            }
-        }
-        {
-            m3 p = adj_mul_adj(load_su3(links, c, storage_index(c, lex_mnpm, par), nu),
-                               load_su3(links, c, storage_index(c, lex_mn, opp), mu));
-            m3 b = mul(p, load_su3(links, c, storage_index(c, lex_mn, opp), nu));
-            add_into(acc, b);
-        }
-    }
-    return acc;
-}
-
-__global__ void __launch_bounds__(kSweepThreads)
-k_su3_metropolis(const ChainInfo *__restrict__ chains, const Tile *__restrict__ tiles,
-                 double2 *__restrict__ links, int parity, int mu, double angle, int uniform,
-                 const uint64_t *__restrict__ sweep_ptr, unsigned long long *__restrict__ accepts) {
-    const Tile tile = tiles[blockIdx.x];
-    const ChainInfo c = chains[tile.chain];
-    const int64_t t = tile.start + threadIdx.x;
-    unsigned accepted = 0;
-    if (t < c.half) {
-        const int64_t s = (int64_t)parity * c.half + t;
-        const Coord x = decode_storage(c, s);
-        const m3 a = staple_sum(links, c, x, parity, mu);
-        m3 u = load_su3_rw(links, c, s, mu);
-        const uint64_t key = link_key(c.seed, *sweep_ptr, x.lex, mu);
-        accepted = visit_link(u, a, c.beta / 3.0, angle, key, uniform);
-        store_su3(links, c, s, mu, u);
-    }
-    const unsigned warp_sum = __reduce_add_sync(0xffffffffu, accepted);
-    if ((threadIdx.x & 31) == 0 && warp_sum) atomicAdd(accepts + tile.chain, (unsigned long long)warp_sum);
-}
-
-__global__ void k_advance_sweep(uint64_t *sweep) { *sweep += 1; }
 
 // ------------------------------------------------------------ reductions
 
@@ -310,13 +55,12 @@ k_su3_plaquette(const ChainInfo *__restrict__ chains, const Tile *__restrict__ t
 #pragma unroll 1
         for (int mu = 0; mu < 3; ++mu) {
             const m3 umu = load_su3(links, c, s, mu);
-            const int64_t lex_pm = shift_lex(c, x.x, x.lex, mu, +1);
-            const int opp = x.par ^ 1;
+            const Nb pm = step(c, x.x, x.lex, x.par, mu, +1);
 #pragma unroll 1
             for (int nu = mu + 1; nu < 4; ++nu) {
-                const int64_t lex_pn = shift_lex(c, x.x, x.lex, nu, +1);
-                m3 p = mul(umu, load_su3(links, c, storage_index(c, lex_pm, opp), nu));
-                p = mul_adj(p, load_su3(links, c, storage_index(c, lex_pn, opp), mu));
+                const Nb pn = step(c, x.x, x.lex, x.par, nu, +1);
+                m3 p = mul(umu, load_su3(links, c, storage_index(c, pm.lex, pm.par), nu));
+                p = mul_adj(p, load_su3(links, c, storage_index(c, pn.lex, pn.par), mu));
                 const double val = retrace_mul_adj(p, load_su3(links, c, s, nu)) / 3.0;
                 v = first ? val : v + val;
                 first = false;
@@ -396,29 +140,6 @@ k_su3_residuals(const ChainInfo *__restrict__ chains, const Tile *__restrict__ t
 }
 
 // ------------------------------------------------------------ reference order
-
-__device__ __forceinline__ m3 generator_rotation_dense(int g, double theta) {
-    m3 r = identity3();
-    if (g == 7) {
-        cplx e1, e2;
-        lambda8_rotation(theta, e1, e2);
-        r.e[0][0] = e1;
-        r.e[1][1] = e1;
-        r.e[2][2] = e2;
-        return r;
-    }
-    double c, s;
-    taylor_chain(0.5 * theta, c, s);
-    const int i0 = g <= 2 ? 0 : (g <= 4 ? 0 : 1);
-    const int i1 = g <= 2 ? 1 : (g <= 4 ? 2 : 2);
-    const int kind = (g == 2) ? 2 : ((g == 1 || g == 4 || g == 6) ? 1 : 0);
-    cplx a, b, cc, d;
-    if (kind == 0) { a = cmake(c, 0); b = cmake(0, s); cc = cmake(0, s); d = cmake(c, 0); }
-    else if (kind == 1) { a = cmake(c, 0); b = cmake(s, 0); cc = cmake(-s, 0); d = cmake(c, 0); }
-    else { a = cmake(c, s); b = cmake(0, 0); cc = cmake(0, 0); d = cmake(c, -s); }
-    r.e[i0][i0] = a; r.e[i0][i1] = b; r.e[i1][i0] = cc; r.e[i1][i1] = d;
-    return r;
-}
 
 __device__ __forceinline__ int64_t lex_of(const ChainInfo &c, const int *x) {
     return ((int64_t)(x[0] * c.n[1] + x[1]) * c.n[2] + x[2]) * c.n[3] + x[3];
@@ -636,22 +357,6 @@ __global__ void k_su3_to_aos(const ChainInfo *__restrict__ chains, int chain,
 
 // ------------------------------------------------------------ launchers
 
-// __constant__ memory is per device: fill it once on every device used.
-static cudaError_t ensure_constants() {
-    static bool done[128] = {};
-    int dev = 0;
-    cudaError_t err = cudaGetDevice(&dev);
-    if (err != cudaSuccess) return err;
-    if (dev < 0 || dev >= 128) return cudaErrorInvalidDevice;
-    if (done[dev]) return cudaSuccess;
-    double inv[68];
-    inv[0] = 0.0;
-    for (int k = 1; k < 68; ++k) inv[k] = 1.0 / (double)k;
-    err = cudaMemcpyToSymbol(c_inv, inv, sizeof inv);
-    if (err == cudaSuccess) done[dev] = true;
-    return err;
-}
-
 static int grid_for(int64_t n, int threads) {
     int64_t b = (n + threads - 1) / threads;
     if (b > 148 * 16) b = 148 * 16;
@@ -678,20 +383,6 @@ cudaError_t launch_su3_to_aos(ym_ensemble *e, int64_t chain) {
     return cudaGetLastError();
 }
 
-cudaError_t launch_su3_metropolis(ym_ensemble *e, int parity, int mu, double angle, int uniform) {
-    cudaError_t err = ensure_constants();
-    if (err != cudaSuccess) return err;
-    k_su3_metropolis<<<(unsigned)e->n_half_tiles, kSweepThreads, 0, e->stream>>>(
-        e->d_chains, e->d_half_tiles, e->d_links, parity, mu, angle, uniform, e->d_sweep,
-        e->d_accepts);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_advance_sweep(ym_ensemble *e) {
-    k_advance_sweep<<<1, 1, 0, e->stream>>>(e->d_sweep);
-    return cudaGetLastError();
-}
-
 cudaError_t launch_su3_plaquette(ym_ensemble *e) {
     k_su3_plaquette<<<(unsigned)e->n_site_tiles, kSiteThreads, 0, e->stream>>>(
         e->d_chains, e->d_site_tiles, e->d_links, e->d_partial);
@@ -711,8 +402,6 @@ cudaError_t launch_su3_residuals(ym_ensemble *e) {
 }
 
 cudaError_t launch_su3_reference_sweeps(ym_ensemble *e, double angle, int64_t n_sweeps) {
-    cudaError_t err = ensure_constants();
-    if (err != cudaSuccess) return err;
     const int threads = 32;
     const int blocks = (int)((e->n_chains + threads - 1) / threads);
     k_su3_reference_sweeps<<<blocks, threads, 0, e->stream>>>(

@@ -144,6 +144,34 @@ __device__ __forceinline__ double retr_row(const cplx *xrow, const m3 &a, int i)
     return (t0 + t1) + t2;
 }
 
+// ---------------------------------------------------------------- fused forms
+//
+// The staple sum and the trace contraction are the engine's own formulation
+// (the reference multiplies out whole plaquettes instead), so they are free
+// to use fused multiply-adds.  Each is a fixed chain of correctly rounded
+// fma() calls, which the CPU oracle repeats with C99 fma() bit for bit.
+
+// acc += a * b, as: re = fma(a.re,b.re,re); re = fma(-a.im,b.im,re);
+//                   im = fma(a.re,b.im,im); im = fma(a.im,b.re,im).
+__device__ __forceinline__ void cfma(cplx &acc, cplx a, cplx b) {
+    acc.re = fma(a.re, b.re, acc.re);
+    acc.re = fma(-a.im, b.im, acc.re);
+    acc.im = fma(a.re, b.im, acc.im);
+    acc.im = fma(a.im, b.re, acc.im);
+}
+
+// Row i of Re Tr(X A): x0.re*A0i.re, then fma(-x0.im, A0i.im), fma(x1.re,
+// A1i.re), fma(-x1.im, A1i.im), fma(x2.re, A2i.re), fma(-x2.im, A2i.im).
+__device__ __forceinline__ double retr_row_fma(const cplx *xrow, const cplx *acol) {
+    double acc = xrow[0].re * acol[0].re;
+    acc = fma(-xrow[0].im, acol[0].im, acc);
+    acc = fma(xrow[1].re, acol[1].re, acc);
+    acc = fma(-xrow[1].im, acol[1].im, acc);
+    acc = fma(xrow[2].re, acol[2].re, acc);
+    acc = fma(-xrow[2].im, acol[2].im, acc);
+    return acc;
+}
+
 // ---------------------------------------------------------------- RNG
 
 constexpr uint64_t kGolden = 0x9E3779B97F4A7C15ULL;
@@ -253,6 +281,20 @@ __device__ __forceinline__ int64_t shift_lex(const ChainInfo &c, const int32_t *
     int64_t st = stride_of(c, d);
     if (dir > 0) return x[d] == c.n[d] - 1 ? lex - (int64_t)(c.n[d] - 1) * st : lex + st;
     return x[d] == 0 ? lex + (int64_t)(c.n[d] - 1) * st : lex - st;
+}
+
+// A neighbouring site: lexicographic index and parity.  A unit step flips the
+// parity, except a periodic wrap across an odd extent (a shift of n-1).
+struct Nb {
+    int64_t lex;
+    int par;
+};
+
+__device__ __forceinline__ Nb step(const ChainInfo &c, const int32_t *x, int64_t lex, int par,
+                                   int d, int dir) {
+    const bool wrap = dir > 0 ? (x[d] == c.n[d] - 1) : (x[d] == 0);
+    const int flip = (wrap && (c.n[d] & 1)) ? 0 : 1;
+    return Nb{shift_lex(c, x, lex, d, dir), par ^ flip};
 }
 
 // SU(3) FP64 link access: plane (mu*9 + entry) of a chain's block.
