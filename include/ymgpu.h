@@ -122,6 +122,29 @@ int32_t ym_su3_reference_average_plaquette(ym_ensemble *ens, double *per_chain);
  * mean over sites and mu<nu of (1/N) Re Tr P, FP64 tree reduction in a fixed
  * order (deterministic; within 1e-15 relative of the sequential sum). */
 int32_t ym_average_plaquette(ym_ensemble *ens, double *per_chain);
+/* Average plaquette without any device allocation.  No counterpart in the
+ * reference: it serves callers that cannot allocate device memory (a host
+ * framework whose pool owns the device and only lends the engine buffers it
+ * allocated itself, or a fixed-footprint deployment that must not call the
+ * CUDA allocator after start-up).
+ *   links   device pointer, 16-byte aligned, to one SU(3) lattice in the
+ *           reference layout (link = site*4+mu, 18 doubles each);
+ *   extents host array of 4 extents, each >= 2;
+ *   out     device pointer receiving one double, the same mean the
+ *           allocating entry point returns (it is not checked for
+ *           finiteness);
+ *   stream  cudaStream_t to enqueue on (NULL: the legacy default stream).
+ * Asynchronous: the value is in `out` once the stream reaches it.  Scratch
+ * is a file-scope device array of 65536 doubles (512 KiB) that every GPU
+ * loading the library holds until exit, so lattices above 8,388,608 sites
+ * fail with YM_ERR_SCRATCH_TOO_SMALL before any device work.  All calls
+ * share that array: calls that overlap on the GPU (concurrent streams or
+ * threads) race and must be serialised by the caller.  The first call on a
+ * device resolves the array's device address for that device; make that
+ * first call before any stream capture. */
+int32_t ym_su3_average_plaquette_noalloc(const double *links, const int64_t *extents,
+                                         double *out, void *stream);
+
 /* Largest unitarity and determinant residual per chain
  * (Su3Lattice4::max_link_*_residual su3_lattice.rs:285-297). */
 int32_t ym_su3_max_residuals(ym_ensemble *ens, double *unitarity, double *determinant);

@@ -46,6 +46,7 @@ SIGNATURES = {
     "ym_su3_max_residuals": [VP, P(f64), P(f64)],
     "ym_ensemble_set_chain": [VP, i64, f64, u64],
     "ym_proposal_angle_from_u64": [u64, f64, P(f64)],
+    "ym_su3_average_plaquette_noalloc": [VP, P(i64), VP, VP],
     "ym_profile_enable": [VP, i32],
     "ym_profile_read": [VP, i32, P(f64), P(i64)],
 }
