@@ -36,7 +36,8 @@ UNIT = "link updates/s"
 EXTENTS = [32, 32, 32, 32]
 BETA = 6.0
 ANGLE = 0.3
-THERMALIZATION = 60
+THERMALIZATION = 400                  # 3/4 at angle 1.0 (fast relaxation), 1/4 at ANGLE
+THERMALIZATION_ANGLE = 1.0
 MASTER_SEED = 0x2C02198105010002
 LINK_BYTES = 144                      # FP64 3x3 complex
 LINKS_PER_UPDATE = 9                  # 8 link reads + 1 write per checkerboard update
@@ -213,7 +214,9 @@ def main():
     links = 4 * volume
     ens = ymgpu.Ensemble([EXTENTS], BETA, seed, lift_reference_caps=True, device=local)
     ens.hot_start()
-    ens.metropolis_sweeps(ANGLE, args.thermalization)
+    wide = (3 * args.thermalization) // 4
+    ens.metropolis_sweeps(THERMALIZATION_ANGLE, wide)
+    ens.metropolis_sweeps(ANGLE, args.thermalization - wide)
     for _ in range(args.warmup):
         ens.metropolis_sweeps(ANGLE, 1)
         ens.average_plaquette()
@@ -298,7 +301,8 @@ def main():
             "data": "synthetic",
             "config": {"workload": "SU(3) 32^4 beta=6.0 plain FP64 Metropolis (configs[2] "
                                    "geometry), 8 ordered hits/link, angle 0.3, Haar hot start "
-                                   f"+ {args.thermalization} thermalization sweeps",
+                                   f"+ {args.thermalization} untimed thermalization sweeps "
+                                   "(3/4 at angle 1.0, 1/4 at 0.3)",
                        "lattice": "32^4", "global_batch": world, "parallelism": f"replicas x{world}",
                        "l2": "inputs 604 MB > 126 MB L2 (no flush)",
                        "step": "1 checkerboard sweep + average plaquette"},
