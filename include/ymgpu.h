@@ -117,6 +117,28 @@ int32_t ym_su3_reference_sweeps(ym_ensemble *ens, double proposal_angle, uint64_
  * reference's summation order (su3_ensemble.rs:228-259), bit for bit. */
 int32_t ym_su3_reference_average_plaquette(ym_ensemble *ens, double *per_chain);
 
+/* ---- SU(2) heat-bath ensemble (su2_ensemble.rs:220-552) ----
+ * n_sweeps Markov sweeps of every chain, each one heat-bath sweep
+ * (checkerboard parity 0 then 1, direction 0..3) followed by
+ * overrelaxation_sweeps overrelaxation sweeps (markov_sweep :465-486).  The
+ * heat-bath sampler is the reference's truncated-exponential inverse CDF with
+ * Haar rejection (su2_ensemble.rs:220-254) or, alternatively, Kennedy-
+ * Pendleton for the same density.  Each link visit draws from its own
+ * counter-based stream; at most max_attempts_per_link proposals per visit,
+ * after which the link keeps its value and the call returns
+ * YM_ERR_HEATBATH_ATTEMPT_LIMIT_EXCEEDED (the device never waits unbounded).
+ * Every extent must be even; beta per chain in [0, 8]. */
+enum { YM_SU2_SAMPLER_REFERENCE = 0, YM_SU2_SAMPLER_KENNEDY_PENDLETON = 1 };
+int32_t ym_su2_markov_sweeps(ym_ensemble *ens, int64_t max_attempts_per_link,
+                             int64_t overrelaxation_sweeps, int32_t sampler, int64_t n_sweeps);
+/* overrelaxation_sweep (su2_ensemble.rs:344-346), checkerboard order. */
+int32_t ym_su2_overrelaxation_sweeps(ym_ensemble *ens, int64_t n_sweeps);
+/* Heat-bath proposals (attempts) and updates per chain since creation or
+ * reset (ChainReport::heatbath_proposals/updates su2_ensemble.rs:180-181). */
+int32_t ym_su2_accounting(ym_ensemble *ens, uint64_t *proposals, uint64_t *updates);
+/* Lattice4::max_link_unit_residual (lib.rs:726-740) per chain. */
+int32_t ym_su2_max_unit_residual(ym_ensemble *ens, double *per_chain);
+
 /* ---- observables ----
  * Average plaquette per chain (su3_ensemble.rs:228 / su2_ensemble.rs:348):
  * mean over sites and mu<nu of (1/N) Re Tr P, FP64 tree reduction in a fixed

@@ -469,3 +469,122 @@ int or_su2_run_chain(const or_su2_config *cfg, double *links_out, double *measur
         return YM_ERR_NON_FINITE_STATISTIC;
     return YM_OK;
 }
+
+/* ------------------------------------------------------ engine order */
+
+/* The engine's SU(2) sweep restated on the CPU (see or_b200.c for the
+ * rationale): checkerboard order, one counter-based SplitMix64 stream per
+ * link visit keyed S(S(seed, sweep), 4*site+mu), S(k, n) = mix64(k+(n+1)g),
+ * with the reference sampler drawing stream words 0, 1, 2, ... in the order
+ * sample_local_heatbath consumes them (su2_ensemble.rs:220-254). */
+static inline uint64_t sm_at(uint64_t seed, uint64_t n) {
+    return or_mix64(seed + (n + 1) * 0x9E3779B97F4A7C15ULL);
+}
+static inline double unit_of(uint64_t w) { return (double)(w >> 11) * (1.0 / 9007199254740992.0); }
+
+static int sample_from_stream(double alpha, uint64_t key, int64_t max_attempts, q4 *out,
+                              uint64_t *attempts) {
+    uint64_t j = 0;
+    double mass = alpha <= ALPHA_ZERO_LIMIT ? 0.0 : -expm1(-2.0 * alpha);
+    for (int64_t a = 1; a <= max_attempts; ++a) {
+        double pu = unit_of(sm_at(key, j++));
+        double r0;
+        if (alpha <= ALPHA_ZERO_LIMIT) {
+            r0 = 2.0 * pu - 1.0;
+        } else {
+            double y = -log1p(-pu * mass) / alpha;
+            r0 = 1.0 - y;
+            if (r0 < -1.0) r0 = -1.0;
+            if (r0 > 1.0) r0 = 1.0;
+        }
+        double radial = sqrt(rmax(1.0 - r0 * r0, 0.0));
+        if (unit_of(sm_at(key, j++)) <= radial) {
+            double z = 2.0 * unit_of(sm_at(key, j++)) - 1.0;
+            double phi = TAU_2PI * unit_of(sm_at(key, j++));
+            double planar = sqrt(rmax(1.0 - z * z, 0.0));
+            double c[4] = {r0, radial * (planar * cos(phi)), radial * (planar * sin(phi)), radial * z};
+            int st = q_from_normalized(c, out);
+            if (st) return st;
+            *attempts = (uint64_t)a;
+            return YM_OK;
+        }
+    }
+    *attempts = (uint64_t)max_attempts;
+    return YM_ERR_HEATBATH_ATTEMPT_LIMIT_EXCEEDED;
+}
+
+int or_su2_cb_sweep(const int64_t *ext, double *links, double beta, uint64_t chain_seed,
+                    uint64_t sweep, int64_t overrelaxation_sweeps, int64_t max_attempts,
+                    uint64_t *proposals) {
+    extents4 e;
+    int st = extents_from(ext, &e, 0, NULL);
+    if (st) return st;
+    for (int i = 0; i < 4; ++i) if (e.n[i] % 2) return YM_ERR_NOT_CHECKERBOARDABLE;
+    uint64_t np = 0;
+    int failed = 0;
+    for (int p = 0; p < 2; ++p)
+        for (int mu = 0; mu < 4; ++mu) {
+            int64_t x[4];
+            for (x[0] = 0; x[0] < e.n[0]; ++x[0])
+                for (x[1] = 0; x[1] < e.n[1]; ++x[1])
+                    for (x[2] = 0; x[2] < e.n[2]; ++x[2])
+                        for (x[3] = 0; x[3] < e.n[3]; ++x[3]) {
+                            if (((x[0] + x[1] + x[2] + x[3]) & 1) != p) continue;
+                            int64_t lex = site_index(&e, x);
+                            double comp[4], norm;
+                            su2_staple(&e, links, x, mu, comp);
+                            st = staple_norm(comp, &norm);
+                            if (st) return st;
+                            q4 r;
+                            uint64_t att = 0;
+                            uint64_t key = sm_at(sm_at(chain_seed, sweep), (uint64_t)(4 * lex + mu));
+                            st = sample_from_stream(beta * norm, key, max_attempts, &r, &att);
+                            np += att;
+                            if (st == YM_ERR_HEATBATH_ATTEMPT_LIMIT_EXCEEDED) { failed = 1; continue; }
+                            if (st) return st;
+                            q4 next = r;
+                            if (norm != 0.0) {
+                                q4 ns;
+                                q_from_normalized(comp, &ns);
+                                next = q_mul(r, q_dagger(ns));
+                            }
+                            q_store(links, lex * 4 + mu, next);
+                        }
+        }
+    for (int64_t k = 0; k < overrelaxation_sweeps; ++k)
+        for (int p = 0; p < 2; ++p)
+            for (int mu = 0; mu < 4; ++mu) {
+                int64_t x[4];
+                for (x[0] = 0; x[0] < e.n[0]; ++x[0])
+                    for (x[1] = 0; x[1] < e.n[1]; ++x[1])
+                        for (x[2] = 0; x[2] < e.n[2]; ++x[2])
+                            for (x[3] = 0; x[3] < e.n[3]; ++x[3]) {
+                                if (((x[0] + x[1] + x[2] + x[3]) & 1) != p) continue;
+                                st = overrelax_link(&e, links, x, mu);
+                                if (st) return st;
+                            }
+            }
+    *proposals = np;
+    return failed ? YM_ERR_HEATBATH_ATTEMPT_LIMIT_EXCEEDED : YM_OK;
+}
+
+/* Overrelaxation only, engine (checkerboard) order. */
+int or_su2_cb_overrelax(const int64_t *ext, double *links) {
+    extents4 e;
+    int st = extents_from(ext, &e, 0, NULL);
+    if (st) return st;
+    for (int i = 0; i < 4; ++i) if (e.n[i] % 2) return YM_ERR_NOT_CHECKERBOARDABLE;
+    for (int p = 0; p < 2; ++p)
+        for (int mu = 0; mu < 4; ++mu) {
+            int64_t x[4];
+            for (x[0] = 0; x[0] < e.n[0]; ++x[0])
+                for (x[1] = 0; x[1] < e.n[1]; ++x[1])
+                    for (x[2] = 0; x[2] < e.n[2]; ++x[2])
+                        for (x[3] = 0; x[3] < e.n[3]; ++x[3]) {
+                            if (((x[0] + x[1] + x[2] + x[3]) & 1) != p) continue;
+                            st = overrelax_link(&e, links, x, mu);
+                            if (st) return st;
+                        }
+        }
+    return YM_OK;
+}

@@ -111,6 +111,10 @@ int or_su2_overrelaxation_sweep(const int64_t *ext, double *links);
 int or_su2_average_plaquette(const int64_t *ext, const double *links, double *out);
 int or_su2_run_chain(const or_su2_config *cfg, double *links_out, double *measurements,
                      or_su2_chain_scalars *out);
+/* Engine update order (checkerboard, per-link counter streams). */
+int or_su2_cb_sweep(const int64_t *ext, double *links, double beta, uint64_t chain_seed,
+                    uint64_t sweep, int64_t overrelaxation_sweeps, int64_t max_attempts,
+                    uint64_t *proposals);
 
 /* SU(3) (su3.rs, su3_lattice.rs, path_holonomy.rs, su3_ensemble.rs) */
 int or_su3_identity(const int64_t *ext, int lift_cap, double *links);

@@ -414,6 +414,15 @@ def su2_overrelaxation_sweep(extents, links) -> None:
     _check(lib().or_su2_overrelaxation_sweep(_ext(extents), _dp(links)), "overrelaxation_sweep")
 
 
+def su2_cb_sweep(extents, links, beta, chain_seed, sweep, overrelaxation_sweeps, max_attempts):
+    p = u64()
+    L = lib()
+    L.or_su2_cb_sweep.argtypes = [P(i64), P(f64), f64, u64, u64, i64, i64, P(u64)]
+    _check(L.or_su2_cb_sweep(_ext(extents), _dp(links), beta, chain_seed, sweep,
+                             overrelaxation_sweeps, max_attempts, C.byref(p)), "su2 cb_sweep")
+    return p.value
+
+
 def su2_run_chain(cfg: dict):
     c = Su2Config()
     c.extents = (i64 * 4)(*cfg["extents"])

@@ -87,6 +87,25 @@ def test_checkerboard_sweeps_bitwise_equal_oracle(oracle, uniform):
     assert np.array_equal(gpu, cpu)
 
 
+def test_graph_replay_equals_direct_launches(oracle):
+    """Batches of >= 8 sweeps replay a captured CUDA graph; the device sweep
+    counter advances on every replay, so 20 sweeps (2 replays + 4 direct)
+    equal the oracle's sweeps 0..19."""
+    import ymgpu
+    ext = [4, 4, 4, 6]
+    start = rough_config(oracle, ext, 8)
+    seed = oracle.derive_su3_chain_seed(MASTER, 21)
+    with ymgpu.Ensemble([ext], 5.7, seed) as ens:
+        ens.upload(0, start)
+        ens.metropolis_sweeps(0.35, 20)
+        gpu = ens.download(0)
+        assert ens.sweep_index == 20
+    cpu = start.copy()
+    for s in range(20):
+        oracle.su3_cb_sweep(ext, cpu, 5.7, 0.35, seed, s)
+    assert np.array_equal(gpu, cpu)
+
+
 def test_uneven_batch_each_chain_equals_oracle(oracle):
     """Chains of different extents, couplings and seeds in one handle."""
     import ymgpu

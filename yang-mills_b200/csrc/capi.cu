@@ -36,8 +36,10 @@ int32_t cuda_status(cudaError_t err) {
 constexpr int64_t kMaxSu3Links = int64_t(1) << 18;   // su3_lattice.rs:17
 constexpr int64_t kMaxSu2Links = int64_t(1) << 20;   // lib.rs:21
 constexpr double kMaxSu3Beta = 12.0;                 // su3_ensemble.rs:24
+constexpr double kMaxSu2Beta = 8.0;                  // su2_ensemble.rs:18
 constexpr double kMinAngle = 1.0e-8;                 // su3_ensemble.rs:27
 constexpr double kMaxAngle = 1.0;                    // su3_ensemble.rs:28
+constexpr int kGraphSweeps = 8;                      // sweeps per captured graph
 
 template <class T>
 cudaError_t dalloc(T **p, size_t count) {
@@ -45,6 +47,7 @@ cudaError_t dalloc(T **p, size_t count) {
 }
 
 void free_all(ym_ensemble *e) {
+    if (e->sweep_graph) cudaGraphExecDestroy(e->sweep_graph);
     for (auto &pool : e->events)
         for (auto &p : pool) {
             cudaEventDestroy(p.start);
@@ -52,7 +55,8 @@ void free_all(ym_ensemble *e) {
         }
     void *ptrs[] = {e->d_chains, e->d_half_tiles, e->d_site_tiles, e->d_site_tile_first,
                     e->d_links, e->d_staging, e->d_partial, e->d_partial2, e->d_result,
-                    e->d_result2, e->d_accepts, e->d_sweep, e->d_rng, e->d_ref_counts};
+                    e->d_result2, e->d_accepts, e->d_sweep, e->d_rng, e->d_ref_counts,
+                    e->d_error};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (e->stream) cudaStreamDestroy(e->stream);
@@ -79,6 +83,25 @@ int32_t require_checkerboard(const ym_ensemble *e) {
 }
 
 int32_t set_device(const ym_ensemble *e) { return cuda_status(cudaSetDevice(e->device)); }
+
+size_t reals_per_link(const ym_ensemble *e) { return e->group == YM_GROUP_SU3 ? 18 : 4; }
+
+cudaError_t identity(ym_ensemble *e) {
+    return e->group == YM_GROUP_SU3 ? ym::launch_su3_identity(e) : ym::launch_su2_identity(e);
+}
+
+// Reads and clears the device error bits of bounded loops that gave up.
+int32_t take_device_error(ym_ensemble *e) {
+    unsigned bits = 0;
+    cudaError_t err = cudaMemcpyAsync(&bits, e->d_error, sizeof bits, cudaMemcpyDeviceToHost, e->stream);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);
+    if (err != cudaSuccess) return cuda_status(err);
+    if (!bits) return YM_OK;
+    err = cudaMemsetAsync(e->d_error, 0, sizeof(unsigned), e->stream);
+    if (err != cudaSuccess) return cuda_status(err);
+    if (bits & 1u) return YM_ERR_HEATBATH_ATTEMPT_LIMIT_EXCEEDED;
+    return YM_ERR_NON_FINITE_STATISTIC;
+}
 
 // Runs `launch` and, when profiling is on, brackets it with an event pair.
 template <class F>
@@ -110,7 +133,7 @@ int32_t ym_ensemble_create(const ym_ensemble_desc *desc, ym_ensemble **out) {
     if (!desc || !out || !desc->extents || !desc->beta || !desc->chain_seed) return YM_ERR_NULL_ARGUMENT;
     *out = nullptr;
     if (desc->n_chains < 1 || desc->n_chains > (int64_t(1) << 30)) return YM_ERR_INVALID_ARGUMENT;
-    if (desc->group != YM_GROUP_SU3) return YM_ERR_WRONG_GROUP;
+    if (desc->group != YM_GROUP_SU3 && desc->group != YM_GROUP_SU2) return YM_ERR_WRONG_GROUP;
     if (desc->precision != YM_PREC_F64) return YM_ERR_UNSUPPORTED_PRECISION;
 
     ym_ensemble *e = new (std::nothrow) ym_ensemble();
@@ -185,6 +208,8 @@ int32_t ym_ensemble_create(const ym_ensemble_desc *desc, ym_ensemble **out) {
     if (err == cudaSuccess) err = dalloc(&e->d_sweep, 1);
     if (err == cudaSuccess) err = dalloc(&e->d_rng, (size_t)e->n_chains);
     if (err == cudaSuccess) err = dalloc(&e->d_ref_counts, 2 * (size_t)e->n_chains);
+    if (err == cudaSuccess) err = dalloc(&e->d_error, 1);
+    if (err == cudaSuccess) err = cudaMemset(e->d_error, 0, sizeof(unsigned));
     if (err == cudaSuccess)
         err = cudaMemcpy(e->d_chains, e->chains.data(), e->chains.size() * sizeof(ChainInfo), cudaMemcpyHostToDevice);
     if (err == cudaSuccess && !half.empty())
@@ -195,7 +220,7 @@ int32_t ym_ensemble_create(const ym_ensemble_desc *desc, ym_ensemble **out) {
         err = cudaMemcpy(e->d_site_tile_first, first.data(), first.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
     if (err == cudaSuccess) err = cudaMemset(e->d_accepts, 0, (size_t)e->n_chains * sizeof(unsigned long long));
     if (err == cudaSuccess) err = cudaMemset(e->d_sweep, 0, sizeof(uint64_t));
-    if (err == cudaSuccess) err = ym::launch_su3_identity(e);
+    if (err == cudaSuccess) err = identity(e);
     if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);
     if (err != cudaSuccess) {
         free_all(e);
@@ -230,7 +255,7 @@ int32_t ym_ensemble_set_identity(ym_ensemble *e) {
     if (!e) return YM_ERR_NULL_ARGUMENT;
     int32_t st = set_device(e);
     if (st) return st;
-    YM_CUDA(ym::launch_su3_identity(e));
+    YM_CUDA(identity(e));
     YM_CUDA(cudaStreamSynchronize(e->stream));
     return YM_OK;
 }
@@ -250,9 +275,9 @@ int32_t ym_ensemble_upload(ym_ensemble *e, int64_t chain, const double *host) {
     if (chain < 0 || chain >= e->n_chains) return YM_ERR_INVALID_ARGUMENT;
     int32_t st = set_device(e);
     if (st) return st;
-    const size_t bytes = (size_t)e->chain_links[chain] * 18 * sizeof(double);
+    const size_t bytes = (size_t)e->chain_links[chain] * reals_per_link(e) * sizeof(double);
     YM_CUDA(cudaMemcpyAsync(e->d_staging, host, bytes, cudaMemcpyHostToDevice, e->stream));
-    YM_CUDA(ym::launch_su3_from_aos(e, chain));
+    YM_CUDA(e->group == YM_GROUP_SU3 ? ym::launch_su3_from_aos(e, chain) : ym::launch_su2_from_aos(e, chain));
     YM_CUDA(cudaStreamSynchronize(e->stream));
     return YM_OK;
 }
@@ -262,8 +287,8 @@ int32_t ym_ensemble_download(ym_ensemble *e, int64_t chain, double *host) {
     if (chain < 0 || chain >= e->n_chains) return YM_ERR_INVALID_ARGUMENT;
     int32_t st = set_device(e);
     if (st) return st;
-    const size_t bytes = (size_t)e->chain_links[chain] * 18 * sizeof(double);
-    YM_CUDA(ym::launch_su3_to_aos(e, chain));
+    const size_t bytes = (size_t)e->chain_links[chain] * reals_per_link(e) * sizeof(double);
+    YM_CUDA(e->group == YM_GROUP_SU3 ? ym::launch_su3_to_aos(e, chain) : ym::launch_su2_to_aos(e, chain));
     YM_CUDA(cudaMemcpyAsync(host, e->d_staging, bytes, cudaMemcpyDeviceToHost, e->stream));
     YM_CUDA(cudaStreamSynchronize(e->stream));
     return YM_OK;
@@ -329,14 +354,40 @@ int32_t ym_su3_metropolis_sweeps(ym_ensemble *e, double angle, int32_t generator
     if (st) return st;
     st = set_device(e);
     if (st) return st;
-    for (int64_t sw = 0; sw < n_sweeps; ++sw) {
+    auto one_sweep = [&]() -> cudaError_t {
         for (int parity = 0; parity < 2; ++parity)
-            for (int mu = 0; mu < 4; ++mu)
-                YM_CUDA(timed(e, YM_KERNEL_SU3_METROPOLIS, [&] {
+            for (int mu = 0; mu < 4; ++mu) {
+                cudaError_t err = timed(e, YM_KERNEL_SU3_METROPOLIS, [&] {
                     return ym::launch_su3_metropolis(e, parity, mu, angle, generator_mode);
-                }));
-        YM_CUDA(ym::launch_advance_sweep(e));
+                });
+                if (err != cudaSuccess) return err;
+            }
+        return ym::launch_advance_sweep(e);
+    };
+    int64_t done = 0;
+    // Batches of kGraphSweeps sweeps replay one captured graph (9 launches
+    // per sweep become one graph launch per batch).  Timed runs launch
+    // directly so each kernel keeps its event pair.
+    if (!e->profiling && n_sweeps >= kGraphSweeps) {
+        if (!e->sweep_graph || e->sweep_graph_angle != angle || e->sweep_graph_mode != generator_mode) {
+            if (e->sweep_graph) cudaGraphExecDestroy(e->sweep_graph);
+            e->sweep_graph = nullptr;
+            cudaGraph_t g = nullptr;
+            YM_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+            cudaError_t err = cudaSuccess;
+            for (int k = 0; k < kGraphSweeps && err == cudaSuccess; ++k) err = one_sweep();
+            cudaError_t end = cudaStreamEndCapture(e->stream, &g);
+            if (err == cudaSuccess) err = end;
+            if (err == cudaSuccess) err = cudaGraphInstantiate(&e->sweep_graph, g, 0);
+            if (g) cudaGraphDestroy(g);
+            YM_CUDA(err);
+            e->sweep_graph_angle = angle;
+            e->sweep_graph_mode = generator_mode;
+        }
+        for (; done + kGraphSweeps <= n_sweeps; done += kGraphSweeps)
+            YM_CUDA(cudaGraphLaunch(e->sweep_graph, e->stream));
     }
+    for (; done < n_sweeps; ++done) YM_CUDA(one_sweep());
     for (int64_t ch = 0; ch < e->n_chains; ++ch)
         e->proposals[ch] += (uint64_t)n_sweeps * 32u * (uint64_t)e->chains[ch].volume;
     return YM_OK;
@@ -344,6 +395,7 @@ int32_t ym_su3_metropolis_sweeps(ym_ensemble *e, double angle, int32_t generator
 
 int32_t ym_su3_accounting(ym_ensemble *e, uint64_t *proposals, uint64_t *accepts) {
     if (!e || !proposals || !accepts) return YM_ERR_NULL_ARGUMENT;
+    if (e->group != YM_GROUP_SU3) return YM_ERR_WRONG_GROUP;
     int32_t st = set_device(e);
     if (st) return st;
     YM_CUDA(cudaMemcpyAsync(accepts, e->d_accepts, (size_t)e->n_chains * sizeof(uint64_t),
@@ -390,6 +442,7 @@ int32_t ym_su3_reference_sweeps(ym_ensemble *e, double angle, uint64_t *rng_stat
 
 int32_t ym_su3_reference_average_plaquette(ym_ensemble *e, double *per_chain) {
     if (!e || !per_chain) return YM_ERR_NULL_ARGUMENT;
+    if (e->group != YM_GROUP_SU3) return YM_ERR_WRONG_GROUP;
     int32_t st = set_device(e);
     if (st) return st;
     YM_CUDA(ym::launch_su3_reference_plaquette(e));
@@ -405,7 +458,11 @@ int32_t ym_average_plaquette(ym_ensemble *e, double *per_chain) {
     if (!e || !per_chain) return YM_ERR_NULL_ARGUMENT;
     int32_t st = set_device(e);
     if (st) return st;
-    YM_CUDA(timed(e, YM_KERNEL_PLAQUETTE, [&] { return ym::launch_su3_plaquette(e); }));
+    YM_CUDA(timed(e, YM_KERNEL_PLAQUETTE, [&] {
+        if (e->group == YM_GROUP_SU3) return ym::launch_su3_plaquette(e);
+        cudaError_t err = ym::launch_su2_plaquette_partials(e);
+        return err == cudaSuccess ? ym::launch_chain_reduce(e, e->d_partial, e->d_result, 0, 6.0) : err;
+    }));
     YM_CUDA(cudaMemcpyAsync(per_chain, e->d_result, (size_t)e->n_chains * sizeof(double),
                             cudaMemcpyDeviceToHost, e->stream));
     YM_CUDA(cudaStreamSynchronize(e->stream));
@@ -416,12 +473,91 @@ int32_t ym_average_plaquette(ym_ensemble *e, double *per_chain) {
 
 int32_t ym_su3_max_residuals(ym_ensemble *e, double *unitarity, double *determinant) {
     if (!e || !unitarity || !determinant) return YM_ERR_NULL_ARGUMENT;
+    if (e->group != YM_GROUP_SU3) return YM_ERR_WRONG_GROUP;
     int32_t st = set_device(e);
     if (st) return st;
     YM_CUDA(ym::launch_su3_residuals(e));
     YM_CUDA(cudaMemcpyAsync(unitarity, e->d_result, (size_t)e->n_chains * sizeof(double),
                             cudaMemcpyDeviceToHost, e->stream));
     YM_CUDA(cudaMemcpyAsync(determinant, e->d_result2, (size_t)e->n_chains * sizeof(double),
+                            cudaMemcpyDeviceToHost, e->stream));
+    YM_CUDA(cudaStreamSynchronize(e->stream));
+    return YM_OK;
+}
+
+// ---- SU(2) ----
+
+int32_t ym_su2_markov_sweeps(ym_ensemble *e, int64_t max_attempts_per_link,
+                             int64_t overrelaxation_sweeps, int32_t sampler, int64_t n_sweeps) {
+    if (!e) return YM_ERR_NULL_ARGUMENT;
+    if (e->group != YM_GROUP_SU2) return YM_ERR_WRONG_GROUP;
+    // heatbath_sweep checks beta, then the attempt limit (su2_ensemble.rs:321-332)
+    for (const ChainInfo &c : e->chains)
+        if (!std::isfinite(c.beta) || c.beta < 0.0 || c.beta > kMaxSu2Beta)
+            return YM_ERR_BETA_OUTSIDE_REFERENCE_RANGE;
+    if (max_attempts_per_link == 0) return YM_ERR_ZERO_HEATBATH_ATTEMPT_LIMIT;
+    if (max_attempts_per_link < 0 || max_attempts_per_link > (int64_t(1) << 30) ||
+        overrelaxation_sweeps < 0 || n_sweeps < 0 || (sampler != YM_SU2_SAMPLER_REFERENCE &&
+                                                      sampler != YM_SU2_SAMPLER_KENNEDY_PENDLETON))
+        return YM_ERR_INVALID_ARGUMENT;
+    int32_t st = require_checkerboard(e);
+    if (st) return st;
+    st = set_device(e);
+    if (st) return st;
+    for (int64_t sw = 0; sw < n_sweeps; ++sw) {
+        for (int parity = 0; parity < 2; ++parity)
+            for (int mu = 0; mu < 4; ++mu)
+                YM_CUDA(timed(e, YM_KERNEL_SU2_HEATBATH, [&] {
+                    return ym::launch_su2_heatbath(e, parity, mu, (int)max_attempts_per_link, sampler);
+                }));
+        YM_CUDA(ym::launch_advance_sweep(e));
+        for (int64_t k = 0; k < overrelaxation_sweeps; ++k)
+            for (int parity = 0; parity < 2; ++parity)
+                for (int mu = 0; mu < 4; ++mu)
+                    YM_CUDA(timed(e, YM_KERNEL_SU2_OVERRELAX, [&] {
+                        return ym::launch_su2_overrelax(e, parity, mu);
+                    }));
+    }
+    for (int64_t ch = 0; ch < e->n_chains; ++ch)
+        e->proposals[ch] += (uint64_t)n_sweeps * 4u * (uint64_t)e->chains[ch].volume;
+    return take_device_error(e);
+}
+
+int32_t ym_su2_overrelaxation_sweeps(ym_ensemble *e, int64_t n_sweeps) {
+    if (!e) return YM_ERR_NULL_ARGUMENT;
+    if (e->group != YM_GROUP_SU2) return YM_ERR_WRONG_GROUP;
+    if (n_sweeps < 0) return YM_ERR_INVALID_ARGUMENT;
+    int32_t st = require_checkerboard(e);
+    if (st) return st;
+    st = set_device(e);
+    if (st) return st;
+    for (int64_t k = 0; k < n_sweeps; ++k)
+        for (int parity = 0; parity < 2; ++parity)
+            for (int mu = 0; mu < 4; ++mu)
+                YM_CUDA(timed(e, YM_KERNEL_SU2_OVERRELAX, [&] { return ym::launch_su2_overrelax(e, parity, mu); }));
+    return take_device_error(e);
+}
+
+int32_t ym_su2_accounting(ym_ensemble *e, uint64_t *proposals, uint64_t *updates) {
+    if (!e || !proposals || !updates) return YM_ERR_NULL_ARGUMENT;
+    if (e->group != YM_GROUP_SU2) return YM_ERR_WRONG_GROUP;
+    int32_t st = set_device(e);
+    if (st) return st;
+    YM_CUDA(cudaMemcpyAsync(proposals, e->d_accepts, (size_t)e->n_chains * sizeof(uint64_t),
+                            cudaMemcpyDeviceToHost, e->stream));
+    YM_CUDA(cudaStreamSynchronize(e->stream));
+    for (int64_t ch = 0; ch < e->n_chains; ++ch) updates[ch] = e->proposals[ch];
+    return YM_OK;
+}
+
+int32_t ym_su2_max_unit_residual(ym_ensemble *e, double *per_chain) {
+    if (!e || !per_chain) return YM_ERR_NULL_ARGUMENT;
+    if (e->group != YM_GROUP_SU2) return YM_ERR_WRONG_GROUP;
+    int32_t st = set_device(e);
+    if (st) return st;
+    YM_CUDA(ym::launch_su2_unit_residual_partials(e));
+    YM_CUDA(ym::launch_chain_reduce(e, e->d_partial, e->d_result, 1, 1.0));
+    YM_CUDA(cudaMemcpyAsync(per_chain, e->d_result, (size_t)e->n_chains * sizeof(double),
                             cudaMemcpyDeviceToHost, e->stream));
     YM_CUDA(cudaStreamSynchronize(e->stream));
     return YM_OK;

@@ -383,6 +383,13 @@ cudaError_t launch_su3_to_aos(ym_ensemble *e, int64_t chain) {
     return cudaGetLastError();
 }
 
+cudaError_t launch_chain_reduce(ym_ensemble *e, const double *partial, double *out, int mode,
+                                double per_site) {
+    k_chain_reduce<<<(unsigned)e->n_chains, 256, 0, e->stream>>>(
+        partial, e->d_site_tile_first, e->d_chains, out, mode, per_site);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_su3_plaquette(ym_ensemble *e) {
     k_su3_plaquette<<<(unsigned)e->n_site_tiles, kSiteThreads, 0, e->stream>>>(
         e->d_chains, e->d_site_tiles, e->d_links, e->d_partial);

@@ -41,13 +41,20 @@ struct ym_ensemble {
     double *d_partial2 = nullptr;          // second partial per site tile
     double *d_result = nullptr;            // n_chains results
     double *d_result2 = nullptr;
-    unsigned long long *d_accepts = nullptr;
+    unsigned long long *d_accepts = nullptr;   // SU(3) accepts / SU(2) heat-bath attempts
+    unsigned *d_error = nullptr;               // device error bits (bounded loops that gave up)
     uint64_t *d_sweep = nullptr;           // next sweep index
     uint64_t *d_rng = nullptr;             // reference-replay stream states
     unsigned long long *d_ref_counts = nullptr;  // reference replay: proposals, accepts
     std::vector<uint64_t> proposals;       // host-counted proposals per chain
 
     cudaStream_t stream = nullptr;
+
+    // Captured batch of sweeps, replayed by ym_su3_metropolis_sweeps (the
+    // sweep index lives in device memory, so every replay advances it).
+    cudaGraphExec_t sweep_graph = nullptr;
+    double sweep_graph_angle = 0.0;
+    int32_t sweep_graph_mode = -1;
 
     // Optional per-kernel timing: event pairs bracket each launch.
     bool profiling = false;
@@ -69,5 +76,16 @@ cudaError_t launch_su3_residuals(ym_ensemble *e);
 cudaError_t launch_su3_reference_sweeps(ym_ensemble *e, double angle, int64_t n_sweeps);
 cudaError_t launch_su3_reference_plaquette(ym_ensemble *e);
 cudaError_t launch_su3_hot_start(ym_ensemble *e);
+cudaError_t launch_chain_reduce(ym_ensemble *e, const double *partial, double *out, int mode,
+                                double per_site);
+
+// su2.cu
+cudaError_t launch_su2_heatbath(ym_ensemble *e, int parity, int mu, int max_attempts, int kp);
+cudaError_t launch_su2_overrelax(ym_ensemble *e, int parity, int mu);
+cudaError_t launch_su2_plaquette_partials(ym_ensemble *e);
+cudaError_t launch_su2_unit_residual_partials(ym_ensemble *e);
+cudaError_t launch_su2_identity(ym_ensemble *e);
+cudaError_t launch_su2_from_aos(ym_ensemble *e, int64_t chain);
+cudaError_t launch_su2_to_aos(ym_ensemble *e, int64_t chain);
 
 }  // namespace ym

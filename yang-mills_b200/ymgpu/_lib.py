@@ -47,6 +47,10 @@ SIGNATURES = {
     "ym_ensemble_set_chain": [VP, i64, f64, u64],
     "ym_proposal_angle_from_u64": [u64, f64, P(f64)],
     "ym_su3_average_plaquette_noalloc": [VP, P(i64), VP, VP],
+    "ym_su2_markov_sweeps": [VP, i64, i64, i32, i64],
+    "ym_su2_overrelaxation_sweeps": [VP, i64],
+    "ym_su2_accounting": [VP, P(u64), P(u64)],
+    "ym_su2_max_unit_residual": [VP, P(f64)],
     "ym_profile_enable": [VP, i32],
     "ym_profile_read": [VP, i32, P(f64), P(i64)],
 }

@@ -85,15 +85,24 @@ class Ensemble:
         check(lib().ym_ensemble_hot_start(self._h), "hot_start")
 
     def upload(self, chain: int, links: np.ndarray) -> None:
-        a = np.ascontiguousarray(links, dtype=np.complex128)
-        if a.size != self.links_in_chain(chain) * 9:
+        """SU(3): (links, 3, 3) complex128; SU(2): (links, 4) float64 quaternions."""
+        if self.group == SU3:
+            a = np.ascontiguousarray(links, dtype=np.complex128)
+            ok = a.size == self.links_in_chain(chain) * 9
+            a = a.view(np.float64)
+        else:
+            a = np.ascontiguousarray(links, dtype=np.float64)
+            ok = a.size == self.links_in_chain(chain) * 4
+        if not ok:
             raise ValueError("link array does not match the chain's extents")
-        check(lib().ym_ensemble_upload(self._h, chain, _f64p(a.view(np.float64))), "upload")
+        check(lib().ym_ensemble_upload(self._h, chain, _f64p(a)), "upload")
 
     def download(self, chain: int, out: np.ndarray | None = None) -> np.ndarray:
         if out is None:
-            out = np.empty((self.links_in_chain(chain), 3, 3), np.complex128)
-        check(lib().ym_ensemble_download(self._h, chain, _f64p(out.view(np.float64))), "download")
+            out = (np.empty((self.links_in_chain(chain), 3, 3), np.complex128) if self.group == SU3
+                   else np.empty((self.links_in_chain(chain), 4), np.float64))
+        buf = out.view(np.float64) if out.dtype == np.complex128 else out
+        check(lib().ym_ensemble_download(self._h, chain, _f64p(buf)), "download")
         return out
 
     def set_chain(self, chain: int, beta: float, seed: int) -> None:
@@ -143,6 +152,29 @@ class Ensemble:
                                             int(n_sweeps), _u64p(p), _u64p(a)),
               "su3_reference_sweeps")
         return st, p, a
+
+    # ------------------------------------------------------------ SU(2) updates
+    def markov_sweeps(self, n_sweeps: int = 1, overrelaxation_sweeps: int = 1,
+                      max_attempts_per_link: int = 10000, sampler: str = "reference") -> None:
+        """Heat-bath + overrelaxation sweeps (su2_ensemble.rs:465-486)."""
+        code = {"reference": 0, "kennedy-pendleton": 1}[sampler]
+        check(lib().ym_su2_markov_sweeps(self._h, int(max_attempts_per_link),
+                                         int(overrelaxation_sweeps), code, int(n_sweeps)),
+              "su2_markov_sweeps")
+
+    def overrelaxation_sweeps(self, n_sweeps: int = 1) -> None:
+        check(lib().ym_su2_overrelaxation_sweeps(self._h, int(n_sweeps)), "su2_overrelaxation")
+
+    def heatbath_accounting(self):
+        p = np.zeros(self.n_chains, np.uint64)
+        u = np.zeros(self.n_chains, np.uint64)
+        check(lib().ym_su2_accounting(self._h, _u64p(p), _u64p(u)), "su2_accounting")
+        return p, u
+
+    def max_unit_residual(self) -> np.ndarray:
+        out = np.zeros(self.n_chains, np.float64)
+        check(lib().ym_su2_max_unit_residual(self._h, _f64p(out)), "su2_max_unit_residual")
+        return out
 
     # ------------------------------------------------------------ timing
     def profile(self, on: bool = True) -> None:

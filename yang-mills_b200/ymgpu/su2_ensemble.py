@@ -89,3 +89,108 @@ def sampling_efficiency(values, log_weights, max_lag, setup, thermalization, sam
                             out.combined_ess_proxy, out.total_cost,
                             out.sampling_cost_per_effective_sample_proxy,
                             out.total_cost_per_effective_sample_proxy)
+
+
+# ---------------------------------------------------------------- SU(2) chains
+
+SAMPLER_ID = "YM-SU2-ENSEMBLE-V1"
+MAX_REFERENCE_BETA = 8.0
+MAX_REFERENCE_SWEEPS = 1 << 20
+MAX_REFERENCE_MEASUREMENTS = 1 << 20
+MAX_OVERRELAXATION_SWEEPS = 16
+MAX_REFERENCE_LINKS = 1 << 20
+
+
+def _err(name: str, where: str):
+    from .errors import VARIANTS, YmError
+    return YmError(VARIANTS[name], where)
+
+
+@dataclass
+class EnsembleConfig:
+    """su2_ensemble.rs:57-107."""
+    extents: tuple
+    beta: float
+    master_seed: int
+    chain_id: int
+    thermalization_sweeps: int
+    measurements: int
+    sweeps_between_measurements: int
+    overrelaxation_sweeps_per_heatbath: int
+    max_heatbath_attempts_per_link: int
+    autocorrelation_max_lag: int
+
+    def validate(self) -> "EnsembleConfig":
+        if not np.isfinite(self.beta) or self.beta < 0.0 or self.beta > MAX_REFERENCE_BETA:
+            raise _err("BetaOutsideReferenceRange", "validate")
+        if self.measurements > MAX_REFERENCE_MEASUREMENTS:
+            raise _err("ScheduleOutsideReferenceRange", "validate")
+        total = self.thermalization_sweeps + self.measurements * self.sweeps_between_measurements
+        if total > MAX_REFERENCE_SWEEPS:
+            raise _err("ScheduleOutsideReferenceRange", "validate")
+        if self.measurements < 2:
+            raise _err("TooFewMeasurements", "validate")
+        if self.sweeps_between_measurements == 0:
+            raise _err("ZeroMeasurementStride", "validate")
+        if self.overrelaxation_sweeps_per_heatbath > MAX_OVERRELAXATION_SWEEPS:
+            raise _err("TooManyOverrelaxationSweeps", "validate")
+        if self.max_heatbath_attempts_per_link == 0:
+            raise _err("ZeroHeatbathAttemptLimit", "validate")
+        if self.autocorrelation_max_lag >= self.measurements:
+            raise _err("AutocorrelationLagOutOfRange", "validate")
+        return self
+
+
+@dataclass
+class ChainReport:
+    """su2_ensemble.rs:172-186."""
+    config: EnsembleConfig
+    derived_seed: int
+    total_heatbath_sweeps: int
+    total_overrelaxation_sweeps: int
+    heatbath_proposals: int
+    heatbath_updates: int
+    mean_heatbath_acceptance: float
+    measurements: np.ndarray
+    diagnostics: ChainDiagnostics
+    final_link_unit_residual: float
+    sampler_id: str = SAMPLER_ID
+    rng_id: str = RNG_ID
+
+
+def run_chains(configs, sampler: str = "reference", device: int = 0):
+    """``run_chain`` (su2_ensemble.rs:488-552) for many chains of one schedule
+    in the same device launches; cold start, heat-bath + overrelaxation."""
+    from .ensemble import SU2, Ensemble
+    for c in configs:
+        c.validate()
+    sched = {(c.thermalization_sweeps, c.measurements, c.sweeps_between_measurements,
+              c.overrelaxation_sweeps_per_heatbath, c.max_heatbath_attempts_per_link)
+             for c in configs}
+    if len(sched) != 1:
+        raise ValueError("run_chains needs one common schedule")
+    therm, nmeas, stride, n_or, attempts = sched.pop()
+    seeds = [derive_chain_seed(c.master_seed, c.chain_id) for c in configs]
+    ens = Ensemble([list(c.extents) for c in configs], [c.beta for c in configs], seeds,
+                   group=SU2, device=device)
+    try:
+        ens.markov_sweeps(therm, n_or, attempts, sampler)
+        meas = np.zeros((len(configs), nmeas))
+        for m in range(nmeas):
+            ens.markov_sweeps(stride, n_or, attempts, sampler)
+            meas[:, m] = ens.average_plaquette()
+        prop, upd = ens.heatbath_accounting()
+        res = ens.max_unit_residual()
+    finally:
+        ens.close()
+    total = therm + nmeas * stride
+    out = []
+    for i, c in enumerate(configs):
+        diag, _ = diagnostics(meas[i], c.autocorrelation_max_lag)
+        out.append(ChainReport(c, seeds[i], total, total * n_or, int(prop[i]), int(upd[i]),
+                               float(upd[i]) / float(prop[i]), meas[i], diag, float(res[i])))
+    return out
+
+
+def run_chain(config: EnsembleConfig, **kw) -> ChainReport:
+    return run_chains([config], **kw)[0]
