@@ -167,6 +167,55 @@ int32_t ym_average_plaquette(ym_ensemble *ens, double *per_chain);
 int32_t ym_su3_average_plaquette_noalloc(const double *links, const int64_t *extents,
                                          double *out, void *stream);
 
+/* Lattice-averaged rectangular Wilson loops: for every chain, every plane
+ * (mu < nu) in the order (0,1),(0,2),(0,3),(1,2),(1,3),(2,3) and every
+ * R <= rmax, T <= tmax (both in 1..4) the mean over start sites of
+ * Re wilson_loop(x, rectangular_path(mu, nu, R, T)) (path_holonomy.rs:172-260;
+ * R steps along mu, T along nu).  out[((chain*6 + plane)*4 + R-1)*4 + T-1];
+ * entries beyond (rmax, tmax) are 0.  The lattice average has no reference
+ * counterpart; each per-site value is the reference's primitive. */
+int32_t ym_su3_wilson_loops(ym_ensemble *ens, int32_t rmax, int32_t tmax, double *out);
+/* Polyakov loop (su3_lattice.rs:185-212) averaged over every start site with
+ * x_dir = 0: out[chain*2 + 0] = mean Re, out[chain*2 + 1] = mean Im. */
+int32_t ym_su3_polyakov_loops(ym_ensemble *ens, int32_t direction, double *out);
+/* scalar_a1pp_operator_basis (glueball_operators.rs:93-160) for every time
+ * slice of every chain: the mean of Re W over the three 1x1 and the six 2x1
+ * spatial orientations and all spatial start sites.  Outputs packed chain by
+ * chain, t = 0..N3-1 (sum over chains of N3 entries each); loop counts are
+ * 3 Vs and 6 Vs.  Needs cubic spatial extents >= 3. */
+int32_t ym_su3_scalar_operator_basis(ym_ensemble *ens, double *plaquette, double *rectangle);
+
+/* ---- transformations between handles of matching geometry ---- */
+int32_t ym_ensemble_copy(ym_ensemble *src, ym_ensemble *dst);
+/* spatial_stout_smear (glueball_smearing.rs:257-268): `levels` synchronous
+ * spatial stout levels of src written to dst (same extents); rho in
+ * (0, 0.25], levels <= 8 unless lift_level_cap (sequential levels compose,
+ * so 10 = 8 then 2 exactly). */
+int32_t ym_su3_spatial_stout_smear(ym_ensemble *src, ym_ensemble *dst, double rho, int64_t levels,
+                                   int32_t lift_level_cap);
+/* spatial_stride2_block (glueball_blocking.rs:105-136): dst holds the
+ * blocked extents (N0/2, N1/2, N2/2, N3) of every src chain. */
+int32_t ym_su3_spatial_stride2_block(ym_ensemble *src, ym_ensemble *dst);
+
+/* ---- connected correlators (host FP64, the reference's order) ----
+ * samples are [configuration][time].
+ * periodic_connected_estimator (glueball_correlators.rs:111-172). */
+int32_t ym_periodic_connected_estimator(const double *samples, int64_t n_configurations,
+                                        int64_t time_extent, double *vacuum_mean, double *raw,
+                                        double *connected);
+/* connected_from_samples (glueball_scalar_production.rs:383-443); omitted < 0
+ * keeps every configuration. */
+int32_t ym_connected_from_samples(const double *samples, int64_t n_configurations,
+                                  int64_t time_extent, int64_t omitted, double *connected);
+/* All delete-one jackknife replicas: replicas[k][tau] = connected_from_samples
+ * omitting configuration k. */
+int32_t ym_jackknife_replicas(const double *samples, int64_t n_configurations, int64_t time_extent,
+                              double *replicas);
+/* jackknife_covariance (glueball_scalar_fit.rs:276-322) over the window
+ * [start, end]; out is (end-start+1)^2 row-major. */
+int32_t ym_jackknife_covariance(const double *replicas, int64_t n_replicas, int64_t time_extent,
+                                int64_t start, int64_t end, double *out);
+
 /* Largest unitarity and determinant residual per chain
  * (Su3Lattice4::max_link_*_residual su3_lattice.rs:285-297). */
 int32_t ym_su3_max_residuals(ym_ensemble *ens, double *unitarity, double *determinant);

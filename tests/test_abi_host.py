@@ -99,3 +99,35 @@ def test_config_validation_fails_closed():
             cfg.validate()
         assert e.value.variant == variant
     Su3EnsembleConfig(**{**base, "extents": [32, 32, 32, 32]}).validate(lift_reference_caps=True)
+
+
+def test_host_correlators_equal_oracle(oracle, golden):
+    """Connected correlators, delete-one jackknife and covariance: the
+    library's host FP64 code equals the oracle bit for bit."""
+    from ymgpu import glueball as G
+    rng = np.random.default_rng(5)
+    s = rng.normal(0.9, 0.02, size=(20, 10))
+    vac, raw, con = G.periodic_connected_estimator(s)
+    ov, oraw, ocon = oracle.periodic_connected_estimator(s)
+    assert vac == ov and np.array_equal(raw, oraw) and np.array_equal(con, ocon)
+    reps = G.jackknife_replicas(s)
+    for k in (0, 7, 19):
+        assert np.array_equal(reps[k], oracle.connected_from_samples(s, k))
+    assert np.array_equal(G.connected_from_samples(s), oracle.connected_from_samples(s))
+    assert np.array_equal(G.jackknife_covariance(reps, 1, 4), oracle.jackknife_covariance(reps, 1, 4))
+    from ymgpu.errors import YmError
+    with pytest.raises(YmError) as e:
+        G.jackknife_covariance(reps[:3], 1, 4)
+    assert e.value.variant == "InsufficientReplicatesForCovariance"
+    with pytest.raises(YmError) as e:
+        G.connected_from_samples(s, 20)
+    assert e.value.variant == "ConfigurationShapeMismatch"
+    # the reference's analytic fixture (glueball_correlators.rs:24-33)
+    v = [x for x in golden["glueball-connected-correlator-phase3c-v1.json"]["vectors"]
+         if x["id"] == "shifted-defect-analytic-correlators"][0]
+    p = np.full((4, 4), 79.0 / 81.0)
+    for c in range(4):
+        p[c, c] = 1.0 - 2.0 / 81.0 + 1.0 / 81.0   # one defect plaquette pair in slice c
+    pv, praw, pcon = G.periodic_connected_estimator(
+        np.array([[0.9753086419753086] * 4] * 4))
+    assert pv == 0.9753086419753086 and np.allclose(pcon, 0.0, atol=1e-15)

@@ -56,7 +56,9 @@ void free_all(ym_ensemble *e) {
     void *ptrs[] = {e->d_chains, e->d_half_tiles, e->d_site_tiles, e->d_site_tile_first,
                     e->d_links, e->d_staging, e->d_partial, e->d_partial2, e->d_result,
                     e->d_result2, e->d_accepts, e->d_sweep, e->d_rng, e->d_ref_counts,
-                    e->d_error};
+                    e->d_error, e->d_obs_partial, e->d_obs_out, e->d_site_vals,
+                    e->d_slice_chain, e->d_slice_t, e->d_slice_plaq, e->d_slice_rect,
+                    e->d_links_tmp};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (e->stream) cudaStreamDestroy(e->stream);
@@ -100,7 +102,55 @@ int32_t take_device_error(ym_ensemble *e) {
     err = cudaMemsetAsync(e->d_error, 0, sizeof(unsigned), e->stream);
     if (err != cudaSuccess) return cuda_status(err);
     if (bits & 1u) return YM_ERR_HEATBATH_ATTEMPT_LIMIT_EXCEEDED;
+    if (bits & 16u) return YM_ERR_NON_FINITE_STAPLE;
+    if (bits & 4u) return YM_ERR_ALGEBRA_PROJECTION_RESIDUAL;
+    if (bits & 8u) return YM_ERR_NON_UNITARY_MATRIX;
     return YM_ERR_NON_FINITE_STATISTIC;
+}
+
+// Measurement scratch (allocated on first use, kept with the handle).
+cudaError_t ensure_obs_scratch(ym_ensemble *e) {
+    if (e->d_obs_partial) return cudaSuccess;
+    int64_t sites = 0;
+    std::vector<int32_t> sc, st;
+    for (int64_t ch = 0; ch < e->n_chains; ++ch) {
+        sites += e->chains[ch].volume;
+        for (int t = 0; t < e->chains[ch].n[3]; ++t) {
+            sc.push_back((int32_t)ch);
+            st.push_back(t);
+        }
+    }
+    e->n_slices = (int64_t)sc.size();
+    cudaError_t err = dalloc(&e->d_obs_partial, (size_t)e->n_site_tiles * 96);
+    if (err == cudaSuccess) err = dalloc(&e->d_obs_out, (size_t)e->n_chains * 96);
+    if (err == cudaSuccess) err = dalloc(&e->d_site_vals, (size_t)sites);
+    if (err == cudaSuccess) err = dalloc(&e->d_slice_chain, sc.size());
+    if (err == cudaSuccess) err = dalloc(&e->d_slice_t, st.size());
+    if (err == cudaSuccess) err = dalloc(&e->d_slice_plaq, sc.size());
+    if (err == cudaSuccess) err = dalloc(&e->d_slice_rect, sc.size());
+    if (err == cudaSuccess)
+        err = cudaMemcpy(e->d_slice_chain, sc.data(), sc.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
+    if (err == cudaSuccess)
+        err = cudaMemcpy(e->d_slice_t, st.data(), st.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
+    return err;
+}
+
+bool same_geometry(const ym_ensemble *a, const ym_ensemble *b) {
+    if (a->n_chains != b->n_chains || a->group != b->group || a->device != b->device) return false;
+    for (int64_t ch = 0; ch < a->n_chains; ++ch)
+        for (int d = 0; d < 4; ++d)
+            if (a->chains[ch].n[d] != b->chains[ch].n[d]) return false;
+    return true;
+}
+
+// glueball_operators.rs:72-91 / glueball_smearing.rs:83-108 spatial checks.
+int32_t require_cubic_spatial(const ym_ensemble *e, int min_extent) {
+    for (const ChainInfo &c : e->chains) {
+        for (int d = 0; d < 3; ++d)
+            if (c.n[d] < min_extent) return YM_ERR_SPATIAL_EXTENT_TOO_SMALL;
+        if (c.n[0] != c.n[1] || c.n[1] != c.n[2]) return YM_ERR_SPATIAL_EXTENTS_NOT_CUBIC;
+    }
+    return YM_OK;
 }
 
 // Runs `launch` and, when profiling is on, brackets it with an event pair.
@@ -483,6 +533,118 @@ int32_t ym_su3_max_residuals(ym_ensemble *e, double *unitarity, double *determin
                             cudaMemcpyDeviceToHost, e->stream));
     YM_CUDA(cudaStreamSynchronize(e->stream));
     return YM_OK;
+}
+
+// ---- observables and transformations ----
+
+int32_t ym_su3_wilson_loops(ym_ensemble *e, int32_t rmax, int32_t tmax, double *out) {
+    if (!e || !out) return YM_ERR_NULL_ARGUMENT;
+    if (e->group != YM_GROUP_SU3) return YM_ERR_WRONG_GROUP;
+    if (rmax == 0 || tmax == 0) return YM_ERR_ZERO_RECTANGLE_EXTENT;   // path_holonomy.rs:233-235
+    if (rmax < 0 || tmax < 0 || rmax > 4 || tmax > 4) return YM_ERR_INVALID_ARGUMENT;
+    int32_t st = set_device(e);
+    if (st) return st;
+    YM_CUDA(ensure_obs_scratch(e));
+    YM_CUDA(timed(e, YM_KERNEL_AUX, [&] { return ym::launch_wilson_loops(e, rmax, tmax, e->d_obs_partial, e->d_obs_out); }));
+    YM_CUDA(cudaMemcpyAsync(out, e->d_obs_out, (size_t)e->n_chains * 96 * sizeof(double),
+                            cudaMemcpyDeviceToHost, e->stream));
+    YM_CUDA(cudaStreamSynchronize(e->stream));
+    return YM_OK;
+}
+
+int32_t ym_su3_polyakov_loops(ym_ensemble *e, int32_t direction, double *out) {
+    if (!e || !out) return YM_ERR_NULL_ARGUMENT;
+    if (e->group != YM_GROUP_SU3) return YM_ERR_WRONG_GROUP;
+    if (direction < 0 || direction >= 4) return YM_ERR_DIRECTION_OUT_OF_RANGE;
+    int32_t st = set_device(e);
+    if (st) return st;
+    YM_CUDA(ensure_obs_scratch(e));
+    YM_CUDA(ym::launch_polyakov(e, direction, e->d_obs_partial, e->d_obs_out));
+    YM_CUDA(cudaMemcpyAsync(out, e->d_obs_out, (size_t)e->n_chains * 2 * sizeof(double),
+                            cudaMemcpyDeviceToHost, e->stream));
+    YM_CUDA(cudaStreamSynchronize(e->stream));
+    return YM_OK;
+}
+
+int32_t ym_su3_scalar_operator_basis(ym_ensemble *e, double *plaquette, double *rectangle) {
+    if (!e || !plaquette || !rectangle) return YM_ERR_NULL_ARGUMENT;
+    if (e->group != YM_GROUP_SU3) return YM_ERR_WRONG_GROUP;
+    int32_t st = require_cubic_spatial(e, 3);
+    if (st) return st;
+    st = set_device(e);
+    if (st) return st;
+    YM_CUDA(ensure_obs_scratch(e));
+    YM_CUDA(timed(e, YM_KERNEL_OPERATORS, [&] {
+        return ym::launch_operator_basis(e, e->d_site_vals, e->d_slice_chain, e->d_slice_t,
+                                         e->n_slices, e->d_slice_plaq, e->d_slice_rect);
+    }));
+    YM_CUDA(cudaMemcpyAsync(plaquette, e->d_slice_plaq, (size_t)e->n_slices * sizeof(double),
+                            cudaMemcpyDeviceToHost, e->stream));
+    YM_CUDA(cudaMemcpyAsync(rectangle, e->d_slice_rect, (size_t)e->n_slices * sizeof(double),
+                            cudaMemcpyDeviceToHost, e->stream));
+    YM_CUDA(cudaStreamSynchronize(e->stream));
+    for (int64_t i = 0; i < e->n_slices; ++i)
+        if (!std::isfinite(plaquette[i]) || !std::isfinite(rectangle[i])) return YM_ERR_NON_FINITE_OBSERVABLE;
+    return YM_OK;
+}
+
+int32_t ym_ensemble_copy(ym_ensemble *src, ym_ensemble *dst) {
+    if (!src || !dst) return YM_ERR_NULL_ARGUMENT;
+    if (!same_geometry(src, dst)) return YM_ERR_LATTICE_EXTENTS_MISMATCH;
+    int32_t st = set_device(dst);
+    if (st) return st;
+    YM_CUDA(cudaStreamSynchronize(src->stream));
+    YM_CUDA(cudaMemcpyAsync(dst->d_links, src->d_links, (size_t)src->total_elems * sizeof(double2),
+                            cudaMemcpyDeviceToDevice, dst->stream));
+    YM_CUDA(cudaStreamSynchronize(dst->stream));
+    return YM_OK;
+}
+
+int32_t ym_su3_spatial_stout_smear(ym_ensemble *src, ym_ensemble *dst, double rho, int64_t levels,
+                                   int32_t lift_level_cap) {
+    if (!src || !dst) return YM_ERR_NULL_ARGUMENT;
+    if (src->group != YM_GROUP_SU3) return YM_ERR_WRONG_GROUP;
+    // validate_parameters (glueball_smearing.rs:83-108), in order
+    if (!std::isfinite(rho)) return YM_ERR_NON_FINITE_RHO;
+    if (rho <= 0.0 || rho > 0.25) return YM_ERR_RHO_OUT_OF_RANGE;
+    if (levels < 0 || (!lift_level_cap && levels > 8)) return YM_ERR_TOO_MANY_LEVELS;
+    int32_t st = require_cubic_spatial(src, 3);
+    if (st) return st;
+    if (!same_geometry(src, dst)) return YM_ERR_LATTICE_EXTENTS_MISMATCH;
+    st = set_device(dst);
+    if (st) return st;
+    if (levels == 0) return ym_ensemble_copy(src, dst);
+    if (!dst->d_links_tmp) YM_CUDA(dalloc(&dst->d_links_tmp, (size_t)dst->total_elems));
+    YM_CUDA(cudaStreamSynchronize(src->stream));
+    const double2 *in = src->d_links;
+    for (int64_t k = 1; k <= levels; ++k) {
+        double2 *out = ((levels - k) % 2 == 0) ? dst->d_links : dst->d_links_tmp;
+        YM_CUDA(timed(dst, YM_KERNEL_STOUT, [&] { return ym::launch_stout_level(dst, in, out, rho); }));
+        in = out;
+    }
+    return take_device_error(dst);
+}
+
+int32_t ym_su3_spatial_stride2_block(ym_ensemble *src, ym_ensemble *dst) {
+    if (!src || !dst) return YM_ERR_NULL_ARGUMENT;
+    if (src->group != YM_GROUP_SU3 || dst->group != YM_GROUP_SU3) return YM_ERR_WRONG_GROUP;
+    // validate_geometry (glueball_blocking.rs:71-83), per chain
+    for (const ChainInfo &c : src->chains) {
+        if (c.n[0] != c.n[1] || c.n[1] != c.n[2]) return YM_ERR_SPATIAL_EXTENTS_NOT_CUBIC;
+        if (c.n[0] < 6) return YM_ERR_SPATIAL_EXTENT_TOO_SMALL;
+        if (c.n[0] % 2 != 0) return YM_ERR_SPATIAL_EXTENT_NOT_EVEN;
+    }
+    if (src->n_chains != dst->n_chains || src->device != dst->device) return YM_ERR_LATTICE_EXTENTS_MISMATCH;
+    for (int64_t ch = 0; ch < src->n_chains; ++ch) {
+        const ChainInfo &f = src->chains[ch], &c = dst->chains[ch];
+        if (c.n[0] * 2 != f.n[0] || c.n[1] * 2 != f.n[1] || c.n[2] * 2 != f.n[2] || c.n[3] != f.n[3])
+            return YM_ERR_LATTICE_EXTENTS_MISMATCH;
+    }
+    int32_t st = set_device(dst);
+    if (st) return st;
+    YM_CUDA(cudaStreamSynchronize(src->stream));
+    YM_CUDA(ym::launch_block(src, dst));
+    return take_device_error(dst);
 }
 
 // ---- SU(2) ----

@@ -162,3 +162,129 @@ int32_t ym_sampling_efficiency(const double *v, int64_t n, const double *log_wei
 }
 
 }  // extern "C"
+
+// ---- connected correlators, jackknife, covariance (host FP64) ----
+
+extern "C" {
+
+// glueball_correlators.rs:111-172
+int32_t ym_periodic_connected_estimator(const double *samples, int64_t ncfg, int64_t nt,
+                                        double *vacuum_mean, double *raw, double *connected) {
+    if (!samples || !vacuum_mean || !raw || !connected) return YM_ERR_NULL_ARGUMENT;
+    if (ncfg < 0 || nt < 0 || (nt > 0 && ncfg > INT64_MAX / nt)) return YM_ERR_SAMPLE_COUNT_OVERFLOW;
+    const int64_t len = ncfg * nt;
+    if (len == 0) return YM_ERR_CORRELATOR_SHAPE_MISMATCH;
+    double ms = 0.0;
+    for (int64_t i = 0; i < len; ++i) {
+        if (!std::isfinite(samples[i])) return YM_ERR_NON_FINITE_OBSERVABLE;
+        ms += samples[i];
+        if (!std::isfinite(ms)) return YM_ERR_NON_FINITE_ACCUMULATOR;
+    }
+    const double mean = ms / (double)len;
+    if (!std::isfinite(mean)) return YM_ERR_NON_FINITE_ACCUMULATOR;
+    const double msq = mean * mean;
+    if (!std::isfinite(msq)) return YM_ERR_NON_FINITE_ACCUMULATOR;
+    for (int64_t tau = 0; tau < nt; ++tau) {
+        double s = 0.0;
+        for (int64_t c = 0; c < ncfg; ++c) {
+            const double *row = samples + c * nt;
+            for (int64_t t = 0; t < nt; ++t) {
+                const double p = row[t] * row[(t + tau) % nt];
+                if (!std::isfinite(p)) return YM_ERR_NON_FINITE_ACCUMULATOR;
+                s += p;
+                if (!std::isfinite(s)) return YM_ERR_NON_FINITE_ACCUMULATOR;
+            }
+        }
+        const double r = s / (double)len;
+        const double cv = r - msq;
+        if (!std::isfinite(r) || !std::isfinite(cv)) return YM_ERR_NON_FINITE_ACCUMULATOR;
+        raw[tau] = r;
+        connected[tau] = cv;
+    }
+    *vacuum_mean = mean;
+    return YM_OK;
+}
+
+// glueball_scalar_production.rs:383-443
+int32_t ym_connected_from_samples(const double *samples, int64_t ncfg, int64_t nt, int64_t omitted,
+                                  double *connected) {
+    if (!samples || !connected) return YM_ERR_NULL_ARGUMENT;
+    if (ncfg <= 0) return YM_ERR_EMPTY_CONFIGURATION_SET;
+    if (nt <= 0) return YM_ERR_CONFIGURATION_SHAPE_MISMATCH;
+    int64_t kept = ncfg;
+    if (omitted >= 0) {
+        if (omitted >= ncfg) return YM_ERR_CONFIGURATION_SHAPE_MISMATCH;
+        kept = ncfg - 1;
+    }
+    if (kept == 0) return YM_ERR_EMPTY_CONFIGURATION_SET;
+    const int64_t count = kept * nt;
+    double ms = 0.0;
+    for (int64_t c = 0; c < ncfg; ++c) {
+        if (c == omitted) continue;
+        for (int64_t t = 0; t < nt; ++t) {
+            const double v = samples[c * nt + t];
+            if (!std::isfinite(v)) return YM_ERR_NON_FINITE_STATISTIC;
+            ms += v;
+        }
+    }
+    const double mean = ms / (double)count;
+    const double msq = mean * mean;
+    if (!std::isfinite(mean) || !std::isfinite(msq)) return YM_ERR_NON_FINITE_STATISTIC;
+    for (int64_t tau = 0; tau < nt; ++tau) {
+        double s = 0.0;
+        for (int64_t c = 0; c < ncfg; ++c) {
+            if (c == omitted) continue;
+            const double *row = samples + c * nt;
+            for (int64_t t = 0; t < nt; ++t) s += row[t] * row[(t + tau) % nt];
+        }
+        const double v = s / (double)count - msq;
+        if (!std::isfinite(v)) return YM_ERR_NON_FINITE_STATISTIC;
+        connected[tau] = v;
+    }
+    return YM_OK;
+}
+
+int32_t ym_jackknife_replicas(const double *samples, int64_t ncfg, int64_t nt, double *replicas) {
+    if (!samples || !replicas) return YM_ERR_NULL_ARGUMENT;
+    for (int64_t k = 0; k < ncfg; ++k) {
+        const int32_t st = ym_connected_from_samples(samples, ncfg, nt, k, replicas + k * nt);
+        if (st) return st;
+    }
+    return ncfg > 0 ? YM_OK : YM_ERR_EMPTY_CONFIGURATION_SET;
+}
+
+// glueball_scalar_fit.rs:276-322
+int32_t ym_jackknife_covariance(const double *replicas, int64_t nrep, int64_t nt, int64_t start,
+                                int64_t end, double *out) {
+    if (!replicas || !out) return YM_ERR_NULL_ARGUMENT;
+    if (start < 0 || end < start) return YM_ERR_INVALID_CANDIDATE_WINDOW;
+    const int64_t points = end - start + 1;
+    if (nrep <= points) return YM_ERR_INSUFFICIENT_REPLICATES_FOR_COVARIANCE;
+    if (end >= nt) return YM_ERR_INVALID_CANDIDATE_WINDOW;
+    std::vector<double> means((size_t)points, 0.0);
+    for (int64_t r = 0; r < nrep; ++r)
+        for (int64_t c = 0; c < points; ++c) {
+            const double v = replicas[r * nt + start + c];
+            if (!std::isfinite(v)) return YM_ERR_NON_FINITE_STATISTIC;
+            means[(size_t)c] += v;
+        }
+    const double n = (double)nrep;
+    for (double &m : means) m /= n;
+    for (int64_t i = 0; i < points * points; ++i) out[i] = 0.0;
+    for (int64_t r = 0; r < nrep; ++r)
+        for (int64_t a = 0; a < points; ++a) {
+            const double left = replicas[r * nt + start + a] - means[(size_t)a];
+            for (int64_t b = 0; b < points; ++b) {
+                const double right = replicas[r * nt + start + b] - means[(size_t)b];
+                out[a * points + b] += left * right;
+            }
+        }
+    const double factor = (n - 1.0) / n;
+    for (int64_t i = 0; i < points * points; ++i) {
+        out[i] *= factor;
+        if (!std::isfinite(out[i])) return YM_ERR_NON_FINITE_STATISTIC;
+    }
+    return YM_OK;
+}
+
+}  // extern "C"

@@ -50,6 +50,17 @@ struct ym_ensemble {
 
     cudaStream_t stream = nullptr;
 
+    // Measurement scratch, allocated on first use.
+    double *d_obs_partial = nullptr;       // n_site_tiles * 96
+    double *d_obs_out = nullptr;           // n_chains * 96
+    double2 *d_site_vals = nullptr;        // one double2 per site
+    int32_t *d_slice_chain = nullptr;      // (chain, t) of every time slice
+    int32_t *d_slice_t = nullptr;
+    double *d_slice_plaq = nullptr;
+    double *d_slice_rect = nullptr;
+    int64_t n_slices = 0;
+    double2 *d_links_tmp = nullptr;        // second link buffer (smearing levels)
+
     // Captured batch of sweeps, replayed by ym_su3_metropolis_sweeps (the
     // sweep index lives in device memory, so every replay advances it).
     cudaGraphExec_t sweep_graph = nullptr;
@@ -78,6 +89,15 @@ cudaError_t launch_su3_reference_plaquette(ym_ensemble *e);
 cudaError_t launch_su3_hot_start(ym_ensemble *e);
 cudaError_t launch_chain_reduce(ym_ensemble *e, const double *partial, double *out, int mode,
                                 double per_site);
+
+// observables.cu / smear.cu
+cudaError_t launch_wilson_loops(ym_ensemble *e, int rmax, int tmax, double *d_partial, double *d_out);
+cudaError_t launch_polyakov(ym_ensemble *e, int dir, double *d_partial, double *d_out);
+cudaError_t launch_operator_basis(ym_ensemble *e, double2 *d_site_vals, const int32_t *d_slice_chain,
+                                  const int32_t *d_slice_t, int64_t n_slices, double *d_plaq,
+                                  double *d_rect);
+cudaError_t launch_stout_level(ym_ensemble *e, const double2 *in, double2 *out, double rho);
+cudaError_t launch_block(ym_ensemble *fine, ym_ensemble *coarse);
 
 // su2.cu
 cudaError_t launch_su2_heatbath(ym_ensemble *e, int parity, int mu, int max_attempts, int kp);

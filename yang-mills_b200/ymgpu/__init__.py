@@ -9,9 +9,9 @@ a compute entry point without the built ``libymgpu.so`` raises.
 from ._lib import LIB_PATH, lib
 from .ensemble import Ensemble, F32_TWO_ROW, F64, ORDERED, SU2, SU3, UNIFORM
 from .errors import YmError
-from . import su2_ensemble, su3_ensemble, su3_lattice
+from . import glueball, su2_ensemble, su3_ensemble, su3_lattice
 from .su3_lattice import Su3Lattice4
 
 __all__ = ["Ensemble", "Su3Lattice4", "YmError", "lib", "LIB_PATH", "su2_ensemble",
-           "su3_ensemble", "su3_lattice", "SU2", "SU3", "F64", "F32_TWO_ROW", "ORDERED",
+           "su3_ensemble", "su3_lattice", "glueball", "SU2", "SU3", "F64", "F32_TWO_ROW", "ORDERED",
            "UNIFORM"]

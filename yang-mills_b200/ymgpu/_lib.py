@@ -47,6 +47,16 @@ SIGNATURES = {
     "ym_ensemble_set_chain": [VP, i64, f64, u64],
     "ym_proposal_angle_from_u64": [u64, f64, P(f64)],
     "ym_su3_average_plaquette_noalloc": [VP, P(i64), VP, VP],
+    "ym_su3_wilson_loops": [VP, i32, i32, P(f64)],
+    "ym_su3_polyakov_loops": [VP, i32, P(f64)],
+    "ym_su3_scalar_operator_basis": [VP, P(f64), P(f64)],
+    "ym_ensemble_copy": [VP, VP],
+    "ym_su3_spatial_stout_smear": [VP, VP, f64, i64, i32],
+    "ym_su3_spatial_stride2_block": [VP, VP],
+    "ym_periodic_connected_estimator": [P(f64), i64, i64, P(f64), P(f64), P(f64)],
+    "ym_connected_from_samples": [P(f64), i64, i64, i64, P(f64)],
+    "ym_jackknife_replicas": [P(f64), i64, i64, P(f64)],
+    "ym_jackknife_covariance": [P(f64), i64, i64, i64, i64, P(f64)],
     "ym_su2_markov_sweeps": [VP, i64, i64, i32, i64],
     "ym_su2_overrelaxation_sweeps": [VP, i64],
     "ym_su2_accounting": [VP, P(u64), P(u64)],

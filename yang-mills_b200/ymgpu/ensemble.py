@@ -51,6 +51,7 @@ class Ensemble:
         self.group = group
         self.precision = precision
         self.n_chains = n
+        self.device = device
 
     # ------------------------------------------------------------ lifetime
     def close(self) -> None:
@@ -193,6 +194,47 @@ class Ensemble:
         out = np.zeros(self.n_chains, np.float64)
         check(lib().ym_average_plaquette(self._h, _f64p(out)), "average_plaquette")
         return out
+
+    def wilson_loops(self, rmax: int = 4, tmax: int = 4) -> np.ndarray:
+        """[chain, plane, R-1, T-1] lattice means of Re W(R x T); planes
+        (0,1),(0,2),(0,3),(1,2),(1,3),(2,3), R along the first direction."""
+        out = np.zeros(self.n_chains * 96, np.float64)
+        check(lib().ym_su3_wilson_loops(self._h, rmax, tmax, _f64p(out)), "wilson_loops")
+        return out.reshape(self.n_chains, 6, 4, 4)
+
+    def polyakov_loops(self, direction: int = 3) -> np.ndarray:
+        out = np.zeros(self.n_chains * 2, np.float64)
+        check(lib().ym_su3_polyakov_loops(self._h, direction, _f64p(out)), "polyakov_loops")
+        return out[0::2] + 1j * out[1::2]
+
+    def scalar_operator_basis(self):
+        """Per chain: (plaquette[t], rectangle[t]) time-slice means."""
+        n = sum(e[3] for e in self.extents)
+        p = np.zeros(n, np.float64)
+        r = np.zeros(n, np.float64)
+        check(lib().ym_su3_scalar_operator_basis(self._h, _f64p(p), _f64p(r)), "operator_basis")
+        out, k = [], 0
+        for e in self.extents:
+            out.append((p[k:k + e[3]].copy(), r[k:k + e[3]].copy()))
+            k += e[3]
+        return out
+
+    def copy_to(self, dst: "Ensemble") -> None:
+        check(lib().ym_ensemble_copy(self._h, dst.handle), "ensemble_copy")
+
+    def stout_smear_into(self, dst: "Ensemble", rho: float, levels: int,
+                         lift_level_cap: bool = False) -> None:
+        check(lib().ym_su3_spatial_stout_smear(self._h, dst.handle, float(rho), int(levels),
+                                               int(lift_level_cap)), "spatial_stout_smear")
+
+    def block_into(self, dst: "Ensemble") -> None:
+        check(lib().ym_su3_spatial_stride2_block(self._h, dst.handle), "spatial_stride2_block")
+
+    def like(self, extents=None) -> "Ensemble":
+        """A new handle with this one's chains (optionally other extents)."""
+        return Ensemble(extents if extents is not None else self.extents, self.beta, self.seeds,
+                        group=self.group, precision=self.precision, lift_reference_caps=True,
+                        device=self.device)
 
     def reference_average_plaquette(self) -> np.ndarray:
         out = np.zeros(self.n_chains, np.float64)
