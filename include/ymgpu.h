@@ -197,6 +197,17 @@ int32_t ym_su3_spatial_stout_smear(ym_ensemble *src, ym_ensemble *dst, double rh
  * blocked extents (N0/2, N1/2, N2/2, N3) of every src chain. */
 int32_t ym_su3_spatial_stride2_block(ym_ensemble *src, ym_ensemble *dst);
 
+/* ---- two-row binary32 storage (YM_PREC_F32_TWO_ROW, no reference
+ * counterpart: the reference stores 18 doubles per link) ----
+ * Gram-Schmidt of every link's two stored rows in binary64, rounded back;
+ * the third row is always rebuilt as conj(row0 x row1). */
+int32_t ym_su3_reunitarize(ym_ensemble *ens);
+/* Copy src into dst of the same extents, converting between YM_PREC_F64 and
+ * YM_PREC_F32_TWO_ROW (binary64 third row rebuilt from the stored rows).
+ * Observables other than the plaquette read binary64 handles; a two-row
+ * chain is measured through such a converted copy. */
+int32_t ym_ensemble_convert(ym_ensemble *src, ym_ensemble *dst);
+
 /* ---- connected correlators (host FP64, the reference's order) ----
  * samples are [configuration][time].
  * periodic_connected_estimator (glueball_correlators.rs:111-172). */

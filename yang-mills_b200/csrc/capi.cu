@@ -88,8 +88,28 @@ int32_t set_device(const ym_ensemble *e) { return cuda_status(cudaSetDevice(e->d
 
 size_t reals_per_link(const ym_ensemble *e) { return e->group == YM_GROUP_SU3 ? 18 : 4; }
 
+bool f32(const ym_ensemble *e) { return e->precision == YM_PREC_F32_TWO_ROW; }
+
 cudaError_t identity(ym_ensemble *e) {
+    if (f32(e)) return ym::launch_f32_identity(e);
     return e->group == YM_GROUP_SU3 ? ym::launch_su3_identity(e) : ym::launch_su2_identity(e);
+}
+
+cudaError_t from_aos(ym_ensemble *e, int64_t chain) {
+    if (f32(e)) return ym::launch_f32_from_aos(e, chain);
+    return e->group == YM_GROUP_SU3 ? ym::launch_su3_from_aos(e, chain) : ym::launch_su2_from_aos(e, chain);
+}
+
+cudaError_t to_aos(ym_ensemble *e, int64_t chain) {
+    if (f32(e)) return ym::launch_f32_to_aos(e, chain);
+    return e->group == YM_GROUP_SU3 ? ym::launch_su3_to_aos(e, chain) : ym::launch_su2_to_aos(e, chain);
+}
+
+// Kernels that read full binary64 SU(3) links.
+int32_t require_su3_f64(const ym_ensemble *e) {
+    if (e->group != YM_GROUP_SU3) return YM_ERR_WRONG_GROUP;
+    if (e->precision != YM_PREC_F64) return YM_ERR_UNSUPPORTED_PRECISION;
+    return YM_OK;
 }
 
 // Reads and clears the device error bits of bounded loops that gave up.
@@ -136,7 +156,9 @@ cudaError_t ensure_obs_scratch(ym_ensemble *e) {
 }
 
 bool same_geometry(const ym_ensemble *a, const ym_ensemble *b) {
-    if (a->n_chains != b->n_chains || a->group != b->group || a->device != b->device) return false;
+    if (a->n_chains != b->n_chains || a->group != b->group || a->device != b->device ||
+        a->precision != b->precision)
+        return false;
     for (int64_t ch = 0; ch < a->n_chains; ++ch)
         for (int d = 0; d < 4; ++d)
             if (a->chains[ch].n[d] != b->chains[ch].n[d]) return false;
@@ -184,7 +206,9 @@ int32_t ym_ensemble_create(const ym_ensemble_desc *desc, ym_ensemble **out) {
     *out = nullptr;
     if (desc->n_chains < 1 || desc->n_chains > (int64_t(1) << 30)) return YM_ERR_INVALID_ARGUMENT;
     if (desc->group != YM_GROUP_SU3 && desc->group != YM_GROUP_SU2) return YM_ERR_WRONG_GROUP;
-    if (desc->precision != YM_PREC_F64) return YM_ERR_UNSUPPORTED_PRECISION;
+    if (desc->precision != YM_PREC_F64 &&
+        !(desc->precision == YM_PREC_F32_TWO_ROW && desc->group == YM_GROUP_SU3))
+        return YM_ERR_UNSUPPORTED_PRECISION;
 
     ym_ensemble *e = new (std::nothrow) ym_ensemble();
     if (!e) return YM_ERR_ALLOCATION_FAILED;
@@ -192,7 +216,9 @@ int32_t ym_ensemble_create(const ym_ensemble_desc *desc, ym_ensemble **out) {
     e->precision = desc->precision;
     e->device = desc->device;
     e->n_chains = desc->n_chains;
-    const int64_t per_link = (e->group == YM_GROUP_SU3) ? 9 : 2;   // double2 per link
+    // storage elements per link: double2 (FP64 SU(3): 9, SU(2): 2) or float2
+    // (two-row binary32 SU(3): 6); chain offsets count those elements
+    const int64_t per_link = e->precision == YM_PREC_F32_TWO_ROW ? 6 : (e->group == YM_GROUP_SU3 ? 9 : 2);
 
     // Lattice4::new_identity / Su3Lattice4::new_identity checks
     // (lib.rs:242-263, su3_lattice.rs:85-106), per chain.
@@ -225,7 +251,8 @@ int32_t ym_ensemble_create(const ym_ensemble_desc *desc, ym_ensemble **out) {
         e->total_links += links;
         if (links > e->max_chain_links) e->max_chain_links = links;
     }
-    e->total_elems = offset;
+    // total_elems counts 16-byte units of link storage
+    e->total_elems = e->precision == YM_PREC_F32_TWO_ROW ? (offset + 1) / 2 : offset;
     e->proposals.assign((size_t)e->n_chains, 0);
 
     // Work tiles: sub-sweeps cover the checkerboard half of every chain,
@@ -315,7 +342,7 @@ int32_t ym_ensemble_hot_start(ym_ensemble *e) {
     if (e->group != YM_GROUP_SU3) return YM_ERR_WRONG_GROUP;
     int32_t st = set_device(e);
     if (st) return st;
-    YM_CUDA(ym::launch_su3_hot_start(e));
+    YM_CUDA(f32(e) ? ym::launch_f32_hot_start(e) : ym::launch_su3_hot_start(e));
     YM_CUDA(cudaStreamSynchronize(e->stream));
     return YM_OK;
 }
@@ -327,7 +354,7 @@ int32_t ym_ensemble_upload(ym_ensemble *e, int64_t chain, const double *host) {
     if (st) return st;
     const size_t bytes = (size_t)e->chain_links[chain] * reals_per_link(e) * sizeof(double);
     YM_CUDA(cudaMemcpyAsync(e->d_staging, host, bytes, cudaMemcpyHostToDevice, e->stream));
-    YM_CUDA(e->group == YM_GROUP_SU3 ? ym::launch_su3_from_aos(e, chain) : ym::launch_su2_from_aos(e, chain));
+    YM_CUDA(from_aos(e, chain));
     YM_CUDA(cudaStreamSynchronize(e->stream));
     return YM_OK;
 }
@@ -338,7 +365,7 @@ int32_t ym_ensemble_download(ym_ensemble *e, int64_t chain, double *host) {
     int32_t st = set_device(e);
     if (st) return st;
     const size_t bytes = (size_t)e->chain_links[chain] * reals_per_link(e) * sizeof(double);
-    YM_CUDA(e->group == YM_GROUP_SU3 ? ym::launch_su3_to_aos(e, chain) : ym::launch_su2_to_aos(e, chain));
+    YM_CUDA(to_aos(e, chain));
     YM_CUDA(cudaMemcpyAsync(host, e->d_staging, bytes, cudaMemcpyDeviceToHost, e->stream));
     YM_CUDA(cudaStreamSynchronize(e->stream));
     return YM_OK;
@@ -408,7 +435,8 @@ int32_t ym_su3_metropolis_sweeps(ym_ensemble *e, double angle, int32_t generator
         for (int parity = 0; parity < 2; ++parity)
             for (int mu = 0; mu < 4; ++mu) {
                 cudaError_t err = timed(e, YM_KERNEL_SU3_METROPOLIS, [&] {
-                    return ym::launch_su3_metropolis(e, parity, mu, angle, generator_mode);
+                    return f32(e) ? ym::launch_f32_metropolis(e, parity, mu, angle, generator_mode)
+                                  : ym::launch_su3_metropolis(e, parity, mu, angle, generator_mode);
                 });
                 if (err != cudaSuccess) return err;
             }
@@ -468,7 +496,7 @@ int32_t ym_reset_accounting(ym_ensemble *e) {
 int32_t ym_su3_reference_sweeps(ym_ensemble *e, double angle, uint64_t *rng_state,
                                 int64_t n_sweeps, uint64_t *proposals, uint64_t *accepts) {
     if (!e || !rng_state) return YM_ERR_NULL_ARGUMENT;
-    if (e->group != YM_GROUP_SU3) return YM_ERR_WRONG_GROUP;
+    { const int32_t g__ = require_su3_f64(e); if (g__) return g__; }
     int32_t st = validate_su3_betas(e);
     if (st) return st;
     st = validate_angle(angle);
@@ -492,7 +520,7 @@ int32_t ym_su3_reference_sweeps(ym_ensemble *e, double angle, uint64_t *rng_stat
 
 int32_t ym_su3_reference_average_plaquette(ym_ensemble *e, double *per_chain) {
     if (!e || !per_chain) return YM_ERR_NULL_ARGUMENT;
-    if (e->group != YM_GROUP_SU3) return YM_ERR_WRONG_GROUP;
+    { const int32_t g__ = require_su3_f64(e); if (g__) return g__; }
     int32_t st = set_device(e);
     if (st) return st;
     YM_CUDA(ym::launch_su3_reference_plaquette(e));
@@ -509,6 +537,10 @@ int32_t ym_average_plaquette(ym_ensemble *e, double *per_chain) {
     int32_t st = set_device(e);
     if (st) return st;
     YM_CUDA(timed(e, YM_KERNEL_PLAQUETTE, [&] {
+        if (f32(e)) {
+            cudaError_t err = ym::launch_f32_plaquette_partials(e);
+            return err == cudaSuccess ? ym::launch_chain_reduce(e, e->d_partial, e->d_result, 0, 6.0) : err;
+        }
         if (e->group == YM_GROUP_SU3) return ym::launch_su3_plaquette(e);
         cudaError_t err = ym::launch_su2_plaquette_partials(e);
         return err == cudaSuccess ? ym::launch_chain_reduce(e, e->d_partial, e->d_result, 0, 6.0) : err;
@@ -523,7 +555,7 @@ int32_t ym_average_plaquette(ym_ensemble *e, double *per_chain) {
 
 int32_t ym_su3_max_residuals(ym_ensemble *e, double *unitarity, double *determinant) {
     if (!e || !unitarity || !determinant) return YM_ERR_NULL_ARGUMENT;
-    if (e->group != YM_GROUP_SU3) return YM_ERR_WRONG_GROUP;
+    { const int32_t g__ = require_su3_f64(e); if (g__) return g__; }
     int32_t st = set_device(e);
     if (st) return st;
     YM_CUDA(ym::launch_su3_residuals(e));
@@ -539,7 +571,7 @@ int32_t ym_su3_max_residuals(ym_ensemble *e, double *unitarity, double *determin
 
 int32_t ym_su3_wilson_loops(ym_ensemble *e, int32_t rmax, int32_t tmax, double *out) {
     if (!e || !out) return YM_ERR_NULL_ARGUMENT;
-    if (e->group != YM_GROUP_SU3) return YM_ERR_WRONG_GROUP;
+    { const int32_t g__ = require_su3_f64(e); if (g__) return g__; }
     if (rmax == 0 || tmax == 0) return YM_ERR_ZERO_RECTANGLE_EXTENT;   // path_holonomy.rs:233-235
     if (rmax < 0 || tmax < 0 || rmax > 4 || tmax > 4) return YM_ERR_INVALID_ARGUMENT;
     int32_t st = set_device(e);
@@ -554,7 +586,7 @@ int32_t ym_su3_wilson_loops(ym_ensemble *e, int32_t rmax, int32_t tmax, double *
 
 int32_t ym_su3_polyakov_loops(ym_ensemble *e, int32_t direction, double *out) {
     if (!e || !out) return YM_ERR_NULL_ARGUMENT;
-    if (e->group != YM_GROUP_SU3) return YM_ERR_WRONG_GROUP;
+    { const int32_t g__ = require_su3_f64(e); if (g__) return g__; }
     if (direction < 0 || direction >= 4) return YM_ERR_DIRECTION_OUT_OF_RANGE;
     int32_t st = set_device(e);
     if (st) return st;
@@ -568,7 +600,7 @@ int32_t ym_su3_polyakov_loops(ym_ensemble *e, int32_t direction, double *out) {
 
 int32_t ym_su3_scalar_operator_basis(ym_ensemble *e, double *plaquette, double *rectangle) {
     if (!e || !plaquette || !rectangle) return YM_ERR_NULL_ARGUMENT;
-    if (e->group != YM_GROUP_SU3) return YM_ERR_WRONG_GROUP;
+    { const int32_t g__ = require_su3_f64(e); if (g__) return g__; }
     int32_t st = require_cubic_spatial(e, 3);
     if (st) return st;
     st = set_device(e);
@@ -603,7 +635,7 @@ int32_t ym_ensemble_copy(ym_ensemble *src, ym_ensemble *dst) {
 int32_t ym_su3_spatial_stout_smear(ym_ensemble *src, ym_ensemble *dst, double rho, int64_t levels,
                                    int32_t lift_level_cap) {
     if (!src || !dst) return YM_ERR_NULL_ARGUMENT;
-    if (src->group != YM_GROUP_SU3) return YM_ERR_WRONG_GROUP;
+    { const int32_t g__ = require_su3_f64(src); if (g__) return g__; }
     // validate_parameters (glueball_smearing.rs:83-108), in order
     if (!std::isfinite(rho)) return YM_ERR_NON_FINITE_RHO;
     if (rho <= 0.0 || rho > 0.25) return YM_ERR_RHO_OUT_OF_RANGE;
@@ -627,7 +659,8 @@ int32_t ym_su3_spatial_stout_smear(ym_ensemble *src, ym_ensemble *dst, double rh
 
 int32_t ym_su3_spatial_stride2_block(ym_ensemble *src, ym_ensemble *dst) {
     if (!src || !dst) return YM_ERR_NULL_ARGUMENT;
-    if (src->group != YM_GROUP_SU3 || dst->group != YM_GROUP_SU3) return YM_ERR_WRONG_GROUP;
+    { const int32_t g__ = require_su3_f64(src); if (g__) return g__; }
+    { const int32_t g__ = require_su3_f64(dst); if (g__) return g__; }
     // validate_geometry (glueball_blocking.rs:71-83), per chain
     for (const ChainInfo &c : src->chains) {
         if (c.n[0] != c.n[1] || c.n[1] != c.n[2]) return YM_ERR_SPATIAL_EXTENTS_NOT_CUBIC;
@@ -645,6 +678,32 @@ int32_t ym_su3_spatial_stride2_block(ym_ensemble *src, ym_ensemble *dst) {
     YM_CUDA(cudaStreamSynchronize(src->stream));
     YM_CUDA(ym::launch_block(src, dst));
     return take_device_error(dst);
+}
+
+int32_t ym_su3_reunitarize(ym_ensemble *e) {
+    if (!e) return YM_ERR_NULL_ARGUMENT;
+    if (e->group != YM_GROUP_SU3) return YM_ERR_WRONG_GROUP;
+    if (!f32(e)) return YM_ERR_UNSUPPORTED_PRECISION;
+    int32_t st = set_device(e);
+    if (st) return st;
+    YM_CUDA(timed(e, YM_KERNEL_AUX, [&] { return ym::launch_f32_reunitarize(e); }));
+    return YM_OK;
+}
+
+int32_t ym_ensemble_convert(ym_ensemble *src, ym_ensemble *dst) {
+    if (!src || !dst) return YM_ERR_NULL_ARGUMENT;
+    if (src->group != YM_GROUP_SU3 || dst->group != YM_GROUP_SU3) return YM_ERR_WRONG_GROUP;
+    if (src->precision == dst->precision) return ym_ensemble_copy(src, dst);
+    if (src->n_chains != dst->n_chains || src->device != dst->device) return YM_ERR_LATTICE_EXTENTS_MISMATCH;
+    for (int64_t ch = 0; ch < src->n_chains; ++ch)
+        for (int d = 0; d < 4; ++d)
+            if (src->chains[ch].n[d] != dst->chains[ch].n[d]) return YM_ERR_LATTICE_EXTENTS_MISMATCH;
+    int32_t st = set_device(dst);
+    if (st) return st;
+    YM_CUDA(cudaStreamSynchronize(src->stream));
+    YM_CUDA(ym::launch_convert(src, dst));
+    YM_CUDA(cudaStreamSynchronize(dst->stream));
+    return YM_OK;
 }
 
 // ---- SU(2) ----

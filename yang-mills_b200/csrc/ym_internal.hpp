@@ -99,6 +99,16 @@ cudaError_t launch_operator_basis(ym_ensemble *e, double2 *d_site_vals, const in
 cudaError_t launch_stout_level(ym_ensemble *e, const double2 *in, double2 *out, double rho);
 cudaError_t launch_block(ym_ensemble *fine, ym_ensemble *coarse);
 
+// su3_f32.cu (two-row binary32 storage)
+cudaError_t launch_f32_metropolis(ym_ensemble *e, int parity, int mu, double angle, int uniform);
+cudaError_t launch_f32_reunitarize(ym_ensemble *e);
+cudaError_t launch_f32_plaquette_partials(ym_ensemble *e);
+cudaError_t launch_f32_identity(ym_ensemble *e);
+cudaError_t launch_f32_hot_start(ym_ensemble *e);
+cudaError_t launch_f32_from_aos(ym_ensemble *e, int64_t chain);
+cudaError_t launch_f32_to_aos(ym_ensemble *e, int64_t chain);
+cudaError_t launch_convert(ym_ensemble *src, ym_ensemble *dst);
+
 // su2.cu
 cudaError_t launch_su2_heatbath(ym_ensemble *e, int parity, int mu, int max_attempts, int kp);
 cudaError_t launch_su2_overrelax(ym_ensemble *e, int parity, int mu);

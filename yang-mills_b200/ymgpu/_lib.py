@@ -57,6 +57,8 @@ SIGNATURES = {
     "ym_connected_from_samples": [P(f64), i64, i64, i64, P(f64)],
     "ym_jackknife_replicas": [P(f64), i64, i64, P(f64)],
     "ym_jackknife_covariance": [P(f64), i64, i64, i64, i64, P(f64)],
+    "ym_su3_reunitarize": [VP],
+    "ym_ensemble_convert": [VP, VP],
     "ym_su2_markov_sweeps": [VP, i64, i64, i32, i64],
     "ym_su2_overrelaxation_sweeps": [VP, i64],
     "ym_su2_accounting": [VP, P(u64), P(u64)],

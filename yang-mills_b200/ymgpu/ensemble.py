@@ -219,6 +219,14 @@ class Ensemble:
             k += e[3]
         return out
 
+    def reunitarize(self) -> None:
+        """Binary64 Gram-Schmidt of two-row binary32 links (YM_PREC_F32_TWO_ROW)."""
+        check(lib().ym_su3_reunitarize(self._h), "reunitarize")
+
+    def convert_to(self, dst: "Ensemble") -> None:
+        """Copy into a handle of the same extents, converting precision."""
+        check(lib().ym_ensemble_convert(self._h, dst.handle), "ensemble_convert")
+
     def copy_to(self, dst: "Ensemble") -> None:
         check(lib().ym_ensemble_copy(self._h, dst.handle), "ensemble_copy")
 
@@ -230,11 +238,13 @@ class Ensemble:
     def block_into(self, dst: "Ensemble") -> None:
         check(lib().ym_su3_spatial_stride2_block(self._h, dst.handle), "spatial_stride2_block")
 
-    def like(self, extents=None) -> "Ensemble":
-        """A new handle with this one's chains (optionally other extents)."""
+    def like(self, extents=None, precision=None) -> "Ensemble":
+        """A new handle with this one's chains (optionally other extents or
+        storage precision)."""
         return Ensemble(extents if extents is not None else self.extents, self.beta, self.seeds,
-                        group=self.group, precision=self.precision, lift_reference_caps=True,
-                        device=self.device)
+                        group=self.group,
+                        precision=self.precision if precision is None else precision,
+                        lift_reference_caps=True, device=self.device)
 
     def reference_average_plaquette(self) -> np.ndarray:
         out = np.zeros(self.n_chains, np.float64)
