@@ -212,59 +212,82 @@ def main():
     seed = ymgpu.su3_ensemble.derive_su3_chain_seed(MASTER_SEED, rank)
     volume = int(np.prod(EXTENTS))
     links = 4 * volume
-    ens = ymgpu.Ensemble([EXTENTS], BETA, seed, lift_reference_caps=True, device=local)
-    ens.hot_start()
-    wide = (3 * args.thermalization) // 4
-    ens.metropolis_sweeps(THERMALIZATION_ANGLE, wide)
-    ens.metropolis_sweeps(ANGLE, args.thermalization - wide)
-    for _ in range(args.warmup):
-        ens.metropolis_sweeps(ANGLE, 1)
-        ens.average_plaquette()
-    ens.synchronize()
-    stream = torch.cuda.ExternalStream(ens.stream(), device=local)
-    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    p0, a0 = ens.accounting()
-    plaq = []
-    ens.profile(True)
-    barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(local) as clocks:
+    peak, peak_kind = measured_peaks()
+
+    def max_over_ranks(x):
+        if world > 1:
+            t = torch.tensor([x], device=f"cuda:{local}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            return float(t.item())
+        return x
+
+    def run_leg(precision, link_bytes, sampler_clocks=False):
+        """Thermalise, then time args.steps steps (sweep [+ reunitarise] +
+        plaquette) with CUDA events on the handle's stream."""
+        ens = ymgpu.Ensemble([EXTENTS], BETA, seed, precision=precision,
+                             lift_reference_caps=True, device=local)
+        ens.hot_start()
+        wide = (3 * args.thermalization) // 4
+        ens.metropolis_sweeps(THERMALIZATION_ANGLE, wide)
+        ens.metropolis_sweeps(ANGLE, args.thermalization - wide)
+        for _ in range(args.warmup):
+            ens.metropolis_sweeps(ANGLE, 1)
+            ens.average_plaquette()
+        ens.synchronize()
+        stream = torch.cuda.ExternalStream(ens.stream(), device=local)
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0, a0 = ens.accounting()
+        plaq = []
+        ens.profile(True)
+        barrier()
+        torch.cuda.synchronize()
+        sampler = ClockSampler(local) if sampler_clocks else None
+        if sampler:
+            sampler.__enter__()
         start.record(stream)
         for _ in range(args.steps):
-            ens.metropolis_sweeps(ANGLE, 1)
+            ens.metropolis_sweeps(ANGLE, 1)     # two-row handles reunitarise inside the sweep
             plaq.append(float(ens.average_plaquette()[0]))
         stop.record(stream)
         stop.synchronize()
         torch.cuda.synchronize()
-    barrier()
-    ms = start.elapsed_time(stop)
-    sweep_ms, sweep_launches = ens.profile_read("su3_metropolis")
-    plaq_ms, plaq_launches = ens.profile_read("plaquette")
-    ens.profile(False)
-    p1, a1 = ens.accounting()
-    if world > 1:
-        t = torch.tensor([ms], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+        if sampler:
+            sampler.__exit__(None, None, None)
+        barrier()
+        ms = max_over_ranks(start.elapsed_time(stop))
+        sweep_ms, sweep_launches = ens.profile_read("su3_metropolis")
+        ens.profile(False)
+        p1, a1 = ens.accounting()
+        # plaquette ESS/s through the reference estimator (su2_ensemble.rs:375-463)
+        max_lag = max(1, min(len(plaq) // 4, 50))
+        diag, _ = diagnostics(np.array(plaq), max_lag)
+        # roofline of the dominant kernel (one checkerboard sub-sweep launch)
+        launch_s = sweep_ms * 1e-3 / max(1, sweep_launches)
+        achieved = (volume // 2) * LINKS_PER_UPDATE * link_bytes / launch_s / 1e9
+        return ens, {
+            "ms": ms, "value": world * links * args.steps / (ms * 1e-3),
+            "plaq": plaq, "diag": diag,
+            "ess_per_s": world * diag.effective_sample_size / (ms * 1e-3),
+            "acceptance": float((a1 - a0)[0]) / float((p1 - p0)[0]),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
+                         "launch_ms": launch_s * 1e3, "kernel_share_of_step": sweep_ms / ms,
+                         "bytes_per_launch": (volume // 2) * LINKS_PER_UPDATE * link_bytes},
+            "clocks": sampler.summary() if sampler else None,
+        }
+
+    # binary32 two-row leg (BASELINE configs[2] link algebra), reported beside
+    f32_ens, f32 = run_leg(ymgpu.F32_TWO_ROW, 48)
+    f32_ens.close()
+    ens, leg = run_leg(ymgpu.F64, LINK_BYTES, sampler_clocks=True)
+    ms, plaq, diag = leg["ms"], leg["plaq"], leg["diag"]
     step_ms = ms / args.steps
-    value = world * links * args.steps / (ms * 1e-3)
-
-    # plaquette ESS/s through the reference estimator (su2_ensemble.rs:375-463)
-    max_lag = max(1, min(len(plaq) // 4, 50))
-    diag, _ = diagnostics(np.array(plaq), max_lag)
-    ess_per_s = world * diag.effective_sample_size / (ms * 1e-3)
-
-    # roofline of the dominant kernel (one checkerboard sub-sweep launch)
-    peak, peak_kind = measured_peaks()
-    launch_s = sweep_ms * 1e-3 / max(1, sweep_launches)
-    bytes_per_launch = (volume // 2) * LINKS_PER_UPDATE * LINK_BYTES
-    achieved = bytes_per_launch / launch_s / 1e9
-    traffic = ncu_traffic_per_launch()
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": traffic,
-                "kernel": "k_su3_metropolis (one checkerboard sub-sweep)",
-                "peak_source": f"{peak_kind} hbm_gbs", "launch_ms": launch_s * 1e3,
-                "kernel_share_of_step": sweep_ms / ms}
+    value = leg["value"]
+    ess_per_s = leg["ess_per_s"]
+    clocks = leg["clocks"]
+    roofline = dict(leg["roofline"])
+    roofline.update({"traffic": ncu_traffic_per_launch(),
+                     "kernel": "k_su3_metropolis (one checkerboard sub-sweep)"})
 
     # end to end through the C ABI with host buffers: upload the lattice from
     # pinned host memory, sweep, measure, download the lattice
@@ -280,11 +303,7 @@ def main():
         ens.average_plaquette()
         ens.download(0, host_np)
     t1 = time.perf_counter()
-    e2e_s = t1 - t0
-    if world > 1:
-        t = torch.tensor([e2e_s], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(t1 - t0)
     e2e = {"value": world * links * e2e_steps / e2e_s, "unit": UNIT,
            "h2d_bytes_per_step": links * LINK_BYTES,
            "d2h_bytes_per_step": links * LINK_BYTES + 8,
@@ -309,10 +328,18 @@ def main():
             "plaquette_mean": float(np.mean(plaq)),
             "plaquette_ess_per_s": ess_per_s,
             "plaquette_tau_int": diag.integrated_autocorrelation_time,
-            "acceptance": float((a1 - a0)[0]) / float((p1 - p0)[0]),
+            "acceptance": leg["acceptance"],
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": int(args.steps * 11),
-            "clocks": clocks.summary(),
+            "clocks": clocks,
+            "fp32_two_row": {
+                "value": f32["value"], "unit": UNIT, "dtype": "f32 links, f64 dS/accept/plaquette",
+                "ms_per_step": f32["ms"] / args.steps,
+                "step": "1 checkerboard sweep + FP64 reunitarisation + average plaquette",
+                "plaquette_mean": float(np.mean(f32["plaq"])),
+                "plaquette_minus_f64": float(np.mean(f32["plaq"]) - np.mean(plaq)),
+                "plaquette_ess_per_s": f32["ess_per_s"], "acceptance": f32["acceptance"],
+                "roofline": f32["roofline"]},
         }
         print(json.dumps(line))
     if world > 1:

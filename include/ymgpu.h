@@ -101,6 +101,13 @@ int32_t ym_ensemble_stream(ym_ensemble *ens, void **stream);
  * beta per chain must lie in [0, 12]. */
 int32_t ym_su3_metropolis_sweeps(ym_ensemble *ens, double proposal_angle, int32_t generator_mode,
                                  int64_t n_sweeps);
+/* The run_chain measurement cadence (su3_ensemble.rs:424-435) without a host
+ * round trip per measurement: n_measurements times {sweeps_per_measurement
+ * sweeps, average plaquette of every chain}, replayed from one captured CUDA
+ * graph; series[m * n_chains + chain] receives measurement m. */
+int32_t ym_su3_measured_sweeps(ym_ensemble *ens, double proposal_angle, int32_t generator_mode,
+                               int64_t n_measurements, int64_t sweeps_per_measurement,
+                               double *series);
 /* Accumulated proposals/accepts per chain since creation or reset
  * (MetropolisAccounting su3_ensemble.rs:117-121). */
 int32_t ym_su3_accounting(ym_ensemble *ens, uint64_t *proposals, uint64_t *accepts);
@@ -187,6 +194,10 @@ int32_t ym_su3_scalar_operator_basis(ym_ensemble *ens, double *plaquette, double
 
 /* ---- transformations between handles of matching geometry ---- */
 int32_t ym_ensemble_copy(ym_ensemble *src, ym_ensemble *dst);
+/* Copy one chain's links into a chain of equal extents, group and precision
+ * of another handle (device to device). */
+int32_t ym_ensemble_copy_chain(ym_ensemble *src, int64_t src_chain, ym_ensemble *dst,
+                               int64_t dst_chain);
 /* spatial_stout_smear (glueball_smearing.rs:257-268): `levels` synchronous
  * spatial stout levels of src written to dst (same extents); rho in
  * (0, 0.25], levels <= 8 unless lift_level_cap (sequential levels compose,
@@ -200,7 +211,9 @@ int32_t ym_su3_spatial_stride2_block(ym_ensemble *src, ym_ensemble *dst);
 /* ---- two-row binary32 storage (YM_PREC_F32_TWO_ROW, no reference
  * counterpart: the reference stores 18 doubles per link) ----
  * Gram-Schmidt of every link's two stored rows in binary64, rounded back;
- * the third row is always rebuilt as conj(row0 x row1). */
+ * the third row is always rebuilt as conj(row0 x row1).  Every sweep of a
+ * two-row handle ends with this step (the representation is unstable
+ * without it); a caller needs it only after uploading foreign links. */
 int32_t ym_su3_reunitarize(ym_ensemble *ens);
 /* Copy src into dst of the same extents, converting between YM_PREC_F64 and
  * YM_PREC_F32_TWO_ROW (binary64 third row rebuilt from the stored rows).

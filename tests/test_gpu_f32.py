@@ -90,10 +90,26 @@ def test_equilibrium_plaquette_fp32_vs_fp64():
             series = np.zeros((nch, 100))
             for m in range(100):
                 ens.metropolis_sweeps(0.35, 2)
-                if prec == ymgpu.F32_TWO_ROW:
-                    ens.reunitarize()
                 series[:, m] = ens.average_plaquette()
         means = series.mean(1)
         res[name] = (means.mean(), means.std(ddof=1) / np.sqrt(nch))
     d = abs(res["f32"][0] - res["f64"][0])
     assert d <= 4.0 * np.hypot(res["f32"][1], res["f64"][1]), res
+
+
+def test_two_row_sweeps_stay_unitary():
+    """Wide proposals for many sweeps: the per-sweep reunitarisation keeps the
+    two-row links on the group (without it the deviation grows geometrically
+    and reaches non-finite values within a few hundred sweeps)."""
+    import ymgpu
+    with ymgpu.Ensemble([[4, 4, 4, 6]] * 8, 6.0, list(range(8)),
+                        precision=ymgpu.F32_TWO_ROW) as e32:
+        e32.hot_start()
+        e32.metropolis_sweeps(1.0, 400)
+        p = e32.average_plaquette()
+        e64 = e32.like(precision=ymgpu.F64)
+        e32.convert_to(e64)
+        u, d = e64.max_residuals()
+        e64.close()
+    assert np.all(np.isfinite(p)) and np.all(p > 0.4)
+    assert np.all(u <= 1e-6) and np.all(d <= 1e-6)

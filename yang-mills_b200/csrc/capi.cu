@@ -48,6 +48,9 @@ cudaError_t dalloc(T **p, size_t count) {
 
 void free_all(ym_ensemble *e) {
     if (e->sweep_graph) cudaGraphExecDestroy(e->sweep_graph);
+    if (e->measure_graph) cudaGraphExecDestroy(e->measure_graph);
+    if (e->d_series) cudaFree(e->d_series);
+    if (e->d_series_row) cudaFree(e->d_series_row);
     for (auto &pool : e->events)
         for (auto &p : pool) {
             cudaEventDestroy(p.start);
@@ -440,6 +443,13 @@ int32_t ym_su3_metropolis_sweeps(ym_ensemble *e, double angle, int32_t generator
                 });
                 if (err != cudaSuccess) return err;
             }
+        // Two-row storage is reunitarised after every sweep: updates that
+        // touch the rebuilt third row feed its norm error back into the
+        // stored rows, so without it the deviation grows geometrically.
+        if (f32(e)) {
+            cudaError_t err = timed(e, YM_KERNEL_AUX, [&] { return ym::launch_f32_reunitarize(e); });
+            if (err != cudaSuccess) return err;
+        }
         return ym::launch_advance_sweep(e);
     };
     int64_t done = 0;
@@ -468,6 +478,74 @@ int32_t ym_su3_metropolis_sweeps(ym_ensemble *e, double angle, int32_t generator
     for (; done < n_sweeps; ++done) YM_CUDA(one_sweep());
     for (int64_t ch = 0; ch < e->n_chains; ++ch)
         e->proposals[ch] += (uint64_t)n_sweeps * 32u * (uint64_t)e->chains[ch].volume;
+    return YM_OK;
+}
+
+int32_t ym_su3_measured_sweeps(ym_ensemble *e, double angle, int32_t generator_mode,
+                               int64_t n_measurements, int64_t sweeps_per_measurement,
+                               double *series) {
+    if (!e || (!series && n_measurements > 0)) return YM_ERR_NULL_ARGUMENT;
+    if (e->group != YM_GROUP_SU3) return YM_ERR_WRONG_GROUP;
+    int32_t st = validate_su3_betas(e);
+    if (st) return st;
+    st = validate_angle(angle);
+    if (st) return st;
+    if (generator_mode != YM_GEN_ORDERED && generator_mode != YM_GEN_UNIFORM) return YM_ERR_INVALID_ARGUMENT;
+    if (n_measurements < 0 || sweeps_per_measurement < 0) return YM_ERR_INVALID_ARGUMENT;
+    st = require_checkerboard(e);
+    if (st) return st;
+    st = set_device(e);
+    if (st) return st;
+    if (n_measurements == 0) return YM_OK;
+    if (e->series_capacity < n_measurements) {
+        if (e->d_series) cudaFree(e->d_series);
+        e->d_series = nullptr;
+        e->series_capacity = 0;
+        YM_CUDA(dalloc(&e->d_series, (size_t)(n_measurements * e->n_chains)));
+        e->series_capacity = n_measurements;
+    }
+    if (!e->d_series_row) YM_CUDA(dalloc(&e->d_series_row, 1));
+    YM_CUDA(cudaMemsetAsync(e->d_series_row, 0, sizeof(uint64_t), e->stream));
+    auto step = [&]() -> cudaError_t {
+        for (int64_t k = 0; k < sweeps_per_measurement; ++k) {
+            for (int parity = 0; parity < 2; ++parity)
+                for (int mu = 0; mu < 4; ++mu) {
+                    cudaError_t err = f32(e) ? ym::launch_f32_metropolis(e, parity, mu, angle, generator_mode)
+                                             : ym::launch_su3_metropolis(e, parity, mu, angle, generator_mode);
+                    if (err != cudaSuccess) return err;
+                }
+            cudaError_t err = f32(e) ? ym::launch_f32_reunitarize(e) : cudaSuccess;
+            if (err == cudaSuccess) err = ym::launch_advance_sweep(e);
+            if (err != cudaSuccess) return err;
+        }
+        cudaError_t err = f32(e) ? ym::launch_f32_plaquette_partials(e) : ym::launch_su3_plaquette(e);
+        if (err == cudaSuccess && f32(e)) err = ym::launch_chain_reduce(e, e->d_partial, e->d_result, 0, 6.0);
+        if (err == cudaSuccess) err = ym::launch_store_series(e, e->d_series, e->d_series_row);
+        return err;
+    };
+    if (!e->measure_graph || e->measure_graph_angle != angle || e->measure_graph_mode != generator_mode ||
+        e->measure_graph_stride != sweeps_per_measurement) {
+        if (e->measure_graph) cudaGraphExecDestroy(e->measure_graph);
+        e->measure_graph = nullptr;
+        cudaGraph_t g = nullptr;
+        YM_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+        cudaError_t err = step();
+        cudaError_t end = cudaStreamEndCapture(e->stream, &g);
+        if (err == cudaSuccess) err = end;
+        if (err == cudaSuccess) err = cudaGraphInstantiate(&e->measure_graph, g, 0);
+        if (g) cudaGraphDestroy(g);
+        YM_CUDA(err);
+        e->measure_graph_angle = angle;
+        e->measure_graph_mode = generator_mode;
+        e->measure_graph_stride = sweeps_per_measurement;
+    }
+    for (int64_t m = 0; m < n_measurements; ++m) YM_CUDA(cudaGraphLaunch(e->measure_graph, e->stream));
+    YM_CUDA(cudaMemcpyAsync(series, e->d_series, (size_t)(n_measurements * e->n_chains) * sizeof(double),
+                            cudaMemcpyDeviceToHost, e->stream));
+    YM_CUDA(cudaStreamSynchronize(e->stream));
+    for (int64_t ch = 0; ch < e->n_chains; ++ch)
+        e->proposals[ch] += (uint64_t)(n_measurements * sweeps_per_measurement) * 32u *
+                            (uint64_t)e->chains[ch].volume;
     return YM_OK;
 }
 
@@ -628,6 +706,29 @@ int32_t ym_ensemble_copy(ym_ensemble *src, ym_ensemble *dst) {
     YM_CUDA(cudaStreamSynchronize(src->stream));
     YM_CUDA(cudaMemcpyAsync(dst->d_links, src->d_links, (size_t)src->total_elems * sizeof(double2),
                             cudaMemcpyDeviceToDevice, dst->stream));
+    YM_CUDA(cudaStreamSynchronize(dst->stream));
+    return YM_OK;
+}
+
+int32_t ym_ensemble_copy_chain(ym_ensemble *src, int64_t src_chain, ym_ensemble *dst,
+                               int64_t dst_chain) {
+    if (!src || !dst) return YM_ERR_NULL_ARGUMENT;
+    if (src_chain < 0 || src_chain >= src->n_chains || dst_chain < 0 || dst_chain >= dst->n_chains)
+        return YM_ERR_INVALID_ARGUMENT;
+    if (src->group != dst->group || src->precision != dst->precision || src->device != dst->device)
+        return YM_ERR_LATTICE_EXTENTS_MISMATCH;
+    const ChainInfo &a = src->chains[src_chain], &b = dst->chains[dst_chain];
+    for (int d = 0; d < 4; ++d)
+        if (a.n[d] != b.n[d]) return YM_ERR_LATTICE_EXTENTS_MISMATCH;
+    int32_t st = set_device(dst);
+    if (st) return st;
+    const size_t elem = f32(src) ? sizeof(float2) : sizeof(double2);
+    const size_t per_link = f32(src) ? 6 : (src->group == YM_GROUP_SU3 ? 9 : 2);
+    const size_t bytes = (size_t)a.volume * 4 * per_link * elem;
+    YM_CUDA(cudaStreamSynchronize(src->stream));
+    YM_CUDA(cudaMemcpyAsync(reinterpret_cast<char *>(dst->d_links) + (size_t)b.offset * elem,
+                            reinterpret_cast<const char *>(src->d_links) + (size_t)a.offset * elem,
+                            bytes, cudaMemcpyDeviceToDevice, dst->stream));
     YM_CUDA(cudaStreamSynchronize(dst->stream));
     return YM_OK;
 }

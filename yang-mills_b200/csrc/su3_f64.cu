@@ -334,6 +334,21 @@ cudaError_t launch_su3_to_aos(ym_ensemble *e, int64_t chain) {
     return cudaGetLastError();
 }
 
+// Appends the per-chain results to row *counter of a device series and
+// advances the counter (one block; replayable inside a graph).
+__global__ void k_store_series(const double *__restrict__ result, double *__restrict__ series,
+                               uint64_t *__restrict__ counter, int n_chains) {
+    const uint64_t row = *counter;
+    for (int c = threadIdx.x; c < n_chains; c += blockDim.x) series[row * n_chains + c] = result[c];
+    __syncthreads();
+    if (threadIdx.x == 0) *counter = row + 1;
+}
+
+cudaError_t launch_store_series(ym_ensemble *e, double *series, uint64_t *counter) {
+    k_store_series<<<1, 256, 0, e->stream>>>(e->d_result, series, counter, (int)e->n_chains);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_chain_reduce(ym_ensemble *e, const double *partial, double *out, int mode,
                                 double per_site) {
     k_chain_reduce<<<(unsigned)e->n_chains, 256, 0, e->stream>>>(

@@ -66,6 +66,14 @@ struct ym_ensemble {
     cudaGraphExec_t sweep_graph = nullptr;
     double sweep_graph_angle = 0.0;
     int32_t sweep_graph_mode = -1;
+    // Captured "sweeps then plaquette into the series" step.
+    cudaGraphExec_t measure_graph = nullptr;
+    double measure_graph_angle = 0.0;
+    int32_t measure_graph_mode = -1;
+    int64_t measure_graph_stride = -1;
+    double *d_series = nullptr;            // [measurement][chain]
+    int64_t series_capacity = 0;           // rows
+    uint64_t *d_series_row = nullptr;
 
     // Optional per-kernel timing: event pairs bracket each launch.
     bool profiling = false;
@@ -89,6 +97,7 @@ cudaError_t launch_su3_reference_plaquette(ym_ensemble *e);
 cudaError_t launch_su3_hot_start(ym_ensemble *e);
 cudaError_t launch_chain_reduce(ym_ensemble *e, const double *partial, double *out, int mode,
                                 double per_site);
+cudaError_t launch_store_series(ym_ensemble *e, double *series, uint64_t *counter);
 
 // observables.cu / smear.cu
 cudaError_t launch_wilson_loops(ym_ensemble *e, int rmax, int tmax, double *d_partial, double *d_out);

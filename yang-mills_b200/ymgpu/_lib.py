@@ -39,6 +39,7 @@ SIGNATURES = {
     "ym_ensemble_stream": [VP, P(VP)],
     "ym_su3_metropolis_sweeps": [VP, f64, i32, i64],
     "ym_su3_accounting": [VP, P(u64), P(u64)],
+    "ym_su3_measured_sweeps": [VP, f64, i32, i64, i64, P(f64)],
     "ym_reset_accounting": [VP],
     "ym_su3_reference_sweeps": [VP, f64, P(u64), i64, P(u64), P(u64)],
     "ym_su3_reference_average_plaquette": [VP, P(f64)],
@@ -51,6 +52,7 @@ SIGNATURES = {
     "ym_su3_polyakov_loops": [VP, i32, P(f64)],
     "ym_su3_scalar_operator_basis": [VP, P(f64), P(f64)],
     "ym_ensemble_copy": [VP, VP],
+    "ym_ensemble_copy_chain": [VP, i64, VP, i64],
     "ym_su3_spatial_stout_smear": [VP, VP, f64, i64, i32],
     "ym_su3_spatial_stride2_block": [VP, VP],
     "ym_periodic_connected_estimator": [P(f64), i64, i64, P(f64), P(f64), P(f64)],

@@ -135,6 +135,15 @@ class Ensemble:
         check(lib().ym_su3_metropolis_sweeps(self._h, float(proposal_angle), _GEN[generator_mode],
                                              int(n_sweeps)), "su3_metropolis_sweeps")
 
+    def measured_sweeps(self, proposal_angle: float, n_measurements: int,
+                        sweeps_per_measurement: int = 1, generator_mode="ordered") -> np.ndarray:
+        """[measurement, chain] plaquette series of a graph-replayed cadence."""
+        out = np.zeros((n_measurements, self.n_chains), np.float64)
+        check(lib().ym_su3_measured_sweeps(self._h, float(proposal_angle), _GEN[generator_mode],
+                                           int(n_measurements), int(sweeps_per_measurement),
+                                           _f64p(out)), "su3_measured_sweeps")
+        return out
+
     def accounting(self):
         p = np.zeros(self.n_chains, np.uint64)
         a = np.zeros(self.n_chains, np.uint64)
@@ -226,6 +235,19 @@ class Ensemble:
     def convert_to(self, dst: "Ensemble") -> None:
         """Copy into a handle of the same extents, converting precision."""
         check(lib().ym_ensemble_convert(self._h, dst.handle), "ensemble_convert")
+
+    def copy_chain_to(self, chain: int, dst: "Ensemble", dst_chain: int) -> None:
+        check(lib().ym_ensemble_copy_chain(self._h, chain, dst.handle, dst_chain), "copy_chain")
+
+    def subset(self, chains) -> "Ensemble":
+        """A new handle holding a device copy of the given chains."""
+        chains = list(chains)
+        out = Ensemble([self.extents[c] for c in chains], self.beta[chains], self.seeds[chains],
+                       group=self.group, precision=self.precision, lift_reference_caps=True,
+                       device=self.device)
+        for j, c in enumerate(chains):
+            self.copy_chain_to(c, out, j)
+        return out
 
     def copy_to(self, dst: "Ensemble") -> None:
         check(lib().ym_ensemble_copy(self._h, dst.handle), "ensemble_copy")
