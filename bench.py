@@ -47,7 +47,7 @@ FALLBACK_HBM_GBS = 6650.0
 def parse():
     ap = argparse.ArgumentParser(description=__doc__)
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--steps", type=int, default=400)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -95,17 +95,36 @@ class ClockSampler:
         self.device = device
         self.proc = None
         self.path = os.path.join("/tmp", f"ym_clocks_{os.getpid()}.csv")
+        self.first = self.last = 0
+
+    def _rows(self):
+        try:
+            with open(self.path) as fh:
+                return [ln for ln in fh.read().splitlines() if ln.count(",") >= 8]
+        except OSError:
+            return []
 
     def __enter__(self):
         try:
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh,
+                 "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.fh,
                 stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
         return self
+
+    def wait_first(self, timeout=5.0):
+        """Block until nvidia-smi has written a sample, so that every later
+        sample falls inside the region that follows."""
+        end = time.time() + timeout
+        while self.proc and time.time() < end and not self._rows():
+            time.sleep(0.02)
+        self.first = len(self._rows())
+
+    def mark_end(self):
+        self.last = len(self._rows())
 
     def __exit__(self, *exc):
         if self.proc:
@@ -119,20 +138,24 @@ class ClockSampler:
     def summary(self):
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        rows = []
-        for line in open(self.path):
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) >= 9:
-                rows.append(parts)
-        if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        rows = [[p.strip() for p in ln.split(",")] for ln in self._rows()]
+        inside = rows[self.first:self.last]
+        if not inside:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"],
+                    "samples": 0}
+
+        def num(v):
+            try:
+                return float(v)
+            except ValueError:
+                return None
+        sm = [num(r[1]) for r in inside if num(r[1]) is not None]
+        mx = [num(r[2]) for r in inside if num(r[2]) is not None]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        reasons = sorted({names[i] for r in inside for i in range(4) if r[5 + i] == "Active"})
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
-                "samples": len(rows)}
+                "samples": len(inside), "interval_ms": 100}
 
 
 def cpu_baseline(seconds_target=12.0):
@@ -244,6 +267,7 @@ def main():
         sampler = ClockSampler(local) if sampler_clocks else None
         if sampler:
             sampler.__enter__()
+            sampler.wait_first()
         start.record(stream)
         for _ in range(args.steps):
             ens.metropolis_sweeps(ANGLE, 1)     # two-row handles reunitarise inside the sweep
@@ -252,6 +276,7 @@ def main():
         stop.synchronize()
         torch.cuda.synchronize()
         if sampler:
+            sampler.mark_end()
             sampler.__exit__(None, None, None)
         barrier()
         ms = max_over_ranks(start.elapsed_time(stop))

@@ -33,6 +33,7 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#include "ym_learned.h"
 #include "ym_status.h"
 
 #ifdef __cplusplus
@@ -292,7 +293,7 @@ int32_t ym_sampling_efficiency(const double *values, int64_t n, const double *lo
  * kernel since the last read, and resets it. */
 enum { YM_KERNEL_SU3_METROPOLIS = 0, YM_KERNEL_PLAQUETTE = 1, YM_KERNEL_SU2_HEATBATH = 2,
        YM_KERNEL_SU2_OVERRELAX = 3, YM_KERNEL_STOUT = 4, YM_KERNEL_OPERATORS = 5,
-       YM_KERNEL_AUX = 6, YM_KERNEL_COUNT = 8 };
+       YM_KERNEL_AUX = 6, YM_KERNEL_LEARNED = 7, YM_KERNEL_COUNT = 8 };
 int32_t ym_profile_enable(ym_ensemble *ens, int32_t on);
 int32_t ym_profile_read(ym_ensemble *ens, int32_t kernel, double *total_ms, int64_t *launches);
 

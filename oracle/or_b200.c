@@ -263,6 +263,34 @@ static void su3_visit(mat3 *u, const mat3 *a, double beta, double angle, uint64_
     }
 }
 
+/* One hit with a given generator: the paired-grid angle of w_angle at half
+ * width `angle` (any positive width; the learned proposal goes beyond the
+ * reference's admissible 1.0), the exact rotation, the binary64 accept test
+ * on the uniform of w_acc. */
+int or_su3_hit(double *u18, const double *a18, double beta, double angle, uint64_t w_angle,
+               uint64_t w_acc, int g, uint64_t *accepted) {
+    if (!(angle > 0.0) || g < 0 || g > 7) return YM_ERR_INVALID_ARGUMENT;
+    mat3 u, a, r, cand;
+    memcpy(&u, u18, sizeof u);
+    memcpy(&a, a18, sizeof a);
+    uint64_t m = w_angle & ((1ULL << 52) - 1);
+    double theta = ((w_angle >> 63) == 0 ? -1.0 : 1.0) * (angle * (double)(2 * m + 1) *
+                                                          (1.0 / 9007199254740992.0));
+    double old_tr = retr_product(&u, &a);
+    or_su3_generator_rotation(g, theta, (double *)&r);
+    cand = rotate_rows(g, &r, &u);
+    double new_tr = retr_product(&cand, &a);
+    double ds = (beta / 3.0) * (old_tr - new_tr);
+    double acc = exp(-fmax(ds, 0.0));
+    double uu = (double)(w_acc >> 11) * (1.0 / 9007199254740992.0);
+    *accepted = 0;
+    if (uu < acc) {
+        memcpy(u18, &cand, sizeof cand);
+        *accepted = 1;
+    }
+    return YM_OK;
+}
+
 /* One checkerboard sweep: parity 0 then 1, direction 0..3 within each. */
 int or_su3_cb_sweep(const int64_t *ext, double *links, double beta, double angle,
                     uint64_t chain_seed, uint64_t sweep, int uniform_generator,

@@ -185,6 +185,26 @@ int or_su3_cb_sweep(const int64_t *ext, double *links, double beta, double angle
                     uint64_t *proposals, uint64_t *accepts);
 int or_su3_plaquette_value(const int64_t *ext, const double *links, const int64_t *x, int mu,
                            int nu, double *out);
+int or_su3_hit(double *u18, const double *a18, double beta, double angle, uint64_t w_angle,
+               uint64_t w_acc, int g, uint64_t *accepted);
+
+/* Learned proposal (or_learned.c) */
+float or_bf16_round(float x);
+int or_lp_features(const double *a18, double beta, double *f16);
+int or_lp_forward(const float *params, const float *x, int64_t n, double *y);
+int or_lp_proposal(const double *y16, double *p8, double *scale);
+int or_lp_objective(const double *y16, const float *m18, double beta, double *e_out, double *dy9);
+int or_lp_loss_grad(const float *params, const float *x, const float *m18, const double *beta,
+                    int64_t n, double *objective, double *grad);
+int or_lp_loss_grad_mode(const float *params, const float *x, const float *m18,
+                         const double *beta, int64_t n, int exact, double *objective,
+                         double *grad);
+int or_lp_retr_rotated(int g, const float *m18, double theta, double *f, double *df);
+int or_lp_objective_exact(const double *params, const double *x, const float *m18,
+                          const double *beta, int64_t n, double *objective);
+int or_lp_pick_generator(uint64_t w, const double *p8);
+int or_lp_cb_sweep(const int64_t *ext, double *links, double beta, const float *params,
+                   uint64_t chain_seed, uint64_t sweep, uint64_t *proposals, uint64_t *accepts);
 
 /* Multi-threaded CPU baseline of the reference Metropolis sweep (or_threads.c) */
 int or_bench_su3_reference(const int64_t *ext, double beta, double angle, uint64_t master_seed,

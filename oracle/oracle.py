@@ -543,3 +543,116 @@ def bench_su3_reference(extents, beta, angle, master_seed, threads, links_per_th
                                         links_per_thread, C.byref(secs), C.byref(done)),
            "bench_su3_reference")
     return secs.value, done.value
+
+
+# ---------------------------------------------------------------- learned proposal
+
+LP_PARAMS = 6288
+LP_OFF = {"W1": 0, "b1": 1024, "W2": 1088, "b2": 5184, "W3": 5248, "b3": 6272}
+
+
+def _f32(a: np.ndarray):
+    assert a.flags["C_CONTIGUOUS"] and a.dtype == np.float32
+    return a.ctypes.data_as(P(C.c_float))
+
+
+def bf16_round(x) -> np.ndarray:
+    """binary32 -> bfloat16 -> binary32, round to nearest even (vectorised)."""
+    a = np.ascontiguousarray(x, np.float32).copy()
+    b = a.view(np.uint32)
+    finite = (b & 0x7F800000) != 0x7F800000
+    r = (b + 0x7FFF + ((b >> 16) & 1)) & 0xFFFF0000
+    b[finite] = r[finite]
+    return a
+
+
+def lp_features(staple18, beta) -> np.ndarray:
+    a = np.ascontiguousarray(staple18, np.complex128)
+    f = np.zeros(16)
+    _check(lib().or_lp_features(_dp(a.view(np.float64)), f64(beta), _dp(f)), "lp_features")
+    return f
+
+
+def lp_forward(params, features) -> np.ndarray:
+    p = np.ascontiguousarray(params, np.float32)
+    x = np.ascontiguousarray(features, np.float32).reshape(-1, 16)
+    y = np.zeros((x.shape[0], 16))
+    L = lib()
+    L.or_lp_forward.argtypes = [P(C.c_float), P(C.c_float), i64, P(f64)]
+    _check(L.or_lp_forward(_f32(p), _f32(x), x.shape[0], _dp(y)), "lp_forward")
+    return y
+
+
+def lp_proposal(y16):
+    y = np.ascontiguousarray(y16, np.float64)
+    p = np.zeros(8)
+    s = f64()
+    _check(lib().or_lp_proposal(_dp(y), _dp(p), C.byref(s)), "lp_proposal")
+    return p, s.value
+
+
+def lp_retr_rotated(g, m18, theta):
+    m = np.ascontiguousarray(m18, np.float32).reshape(18)
+    f, df = f64(), f64()
+    L = lib()
+    L.or_lp_retr_rotated.argtypes = [C.c_int, P(C.c_float), f64, P(f64), P(f64)]
+    _check(L.or_lp_retr_rotated(g, _f32(m), theta, C.byref(f), C.byref(df)), "lp_retr_rotated")
+    return f.value, df.value
+
+
+def lp_loss_grad(params, features, m18, beta, exact=False):
+    """Objective and gradient with the device's BF16 roundings (exact=False)
+    or in plain binary64 arithmetic on binary32 inputs (exact=True)."""
+    p = np.ascontiguousarray(params, np.float32)
+    x = np.ascontiguousarray(features, np.float32).reshape(-1, 16)
+    m = np.ascontiguousarray(m18, np.float32).reshape(-1, 18)
+    b = np.ascontiguousarray(np.broadcast_to(np.asarray(beta, np.float64), (x.shape[0],)))
+    g = np.zeros(LP_PARAMS)
+    obj = f64()
+    L = lib()
+    L.or_lp_loss_grad_mode.argtypes = [P(C.c_float), P(C.c_float), P(C.c_float), P(f64), i64,
+                                       C.c_int, P(f64), P(f64)]
+    _check(L.or_lp_loss_grad_mode(_f32(p), _f32(x), _f32(m), _dp(b), x.shape[0], int(exact),
+                                  C.byref(obj), _dp(g)), "lp_loss_grad")
+    return obj.value, g
+
+
+def lp_objective_exact(params, features, m18, beta) -> float:
+    p = np.ascontiguousarray(params, np.float64)
+    x = np.ascontiguousarray(features, np.float64).reshape(-1, 16)
+    m = np.ascontiguousarray(m18, np.float32).reshape(-1, 18)
+    b = np.ascontiguousarray(np.broadcast_to(np.asarray(beta, np.float64), (x.shape[0],)))
+    obj = f64()
+    L = lib()
+    L.or_lp_objective_exact.argtypes = [P(f64), P(f64), P(C.c_float), P(f64), i64, P(f64)]
+    _check(L.or_lp_objective_exact(_dp(p), _dp(x), _f32(m), _dp(b), x.shape[0], C.byref(obj)),
+           "lp_objective_exact")
+    return obj.value
+
+
+def lp_pick_generator(word, p8) -> int:
+    p = np.ascontiguousarray(p8, np.float64)
+    L = lib()
+    L.or_lp_pick_generator.argtypes = [u64, P(f64)]
+    return int(L.or_lp_pick_generator(word, _dp(p)))
+
+
+def lp_cb_sweep(extents, links, beta, params, chain_seed, sweep):
+    p = np.ascontiguousarray(params, np.float32)
+    npr, nac = u64(), u64()
+    L = lib()
+    L.or_lp_cb_sweep.argtypes = [P(i64), P(f64), f64, P(C.c_float), u64, u64, P(u64), P(u64)]
+    _check(L.or_lp_cb_sweep(_ext(extents), _dp(links.view(np.float64)), beta, _f32(p), chain_seed,
+                            sweep, C.byref(npr), C.byref(nac)), "lp_cb_sweep")
+    return npr.value, nac.value
+
+
+def su3_hit(u18, staple18, beta, angle, w_angle, w_acc, g):
+    u = np.ascontiguousarray(u18, np.complex128).copy()
+    a = np.ascontiguousarray(staple18, np.complex128)
+    acc = u64()
+    L = lib()
+    L.or_su3_hit.argtypes = [P(f64), P(f64), f64, f64, u64, u64, C.c_int, P(u64)]
+    _check(L.or_su3_hit(_dp(u.view(np.float64)), _dp(a.view(np.float64)), beta, angle, w_angle,
+                        w_acc, g, C.byref(acc)), "su3_hit")
+    return u, bool(acc.value)

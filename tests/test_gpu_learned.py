@@ -1,0 +1,139 @@
+"""The learned proposal on the device against the oracle: tensor-core
+forward, objective and gradient, training records, and the learned sweep;
+then what training buys over plain Metropolis at equal plaquette.
+
+Tolerances: the device network accumulates in FP32 where the oracle sums in
+binary64 over the same BF16-rounded operands, so an activation can land on
+the other side of a BF16 rounding boundary; outputs agree to 2e-3 (relative
+to max(1, |y|)), gradients to 3% of their norm, the objective to 1e-4
+relative.  Features and M = U A come from binary32 staples: 2e-5 of their
+scale."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def thermal_f32(extents, n_chains, sweeps=60, beta=6.0, seed=7):
+    import ymgpu
+    from ymgpu.su3_ensemble import derive_su3_chain_seed
+    seeds = [derive_su3_chain_seed(seed, i) for i in range(n_chains)]
+    ens = ymgpu.Ensemble([extents] * n_chains, beta, seeds, precision=ymgpu.F32_TWO_ROW,
+                         lift_reference_caps=True)
+    ens.hot_start()
+    ens.metropolis_sweeps(0.8, sweeps, "uniform")
+    return ens
+
+
+def test_forward_matches_oracle(oracle):
+    import ymgpu
+    rng = np.random.default_rng(1)
+    with thermal_f32([4, 4, 4, 6], 2) as ens, ymgpu.ProposalModel(seed=99) as model:
+        f, _, _ = ymgpu.learned.records(ens, 1, 2)
+        x = np.concatenate([f, rng.standard_normal((77, 16)).astype(np.float32)])
+        p = model.params
+        p[6272:6281] = rng.standard_normal(9) * 0.5      # non-trivial output biases
+        p[5248:5248 + 9 * 64] *= 8.0
+        model.params = p
+        y = model.forward(x)
+        ref = oracle.lp_forward(model.params, x)
+    assert y.shape == (x.shape[0], 16)
+    assert np.all(y[:, 9:] == 0)
+    err = np.abs(y - ref) / np.maximum(1.0, np.abs(ref))
+    assert err.max() <= 2e-3, err.max()
+
+
+def test_records_match_oracle(oracle):
+    import ymgpu
+    ext = [4, 4, 4, 4]
+    with thermal_f32(ext, 1) as ens:
+        links = ens.download(0)
+        for parity, mu in ((0, 0), (1, 3)):
+            f, m, b = ymgpu.learned.records(ens, parity, mu)
+            assert f.shape == (128, 16) and np.all(b == 6.0)
+            for t in range(0, 128, 9):
+                lex = 2 * t
+                x = [lex // 64, (lex // 16) % 4, (lex // 4) % 4, lex % 4]
+                if sum(x) % 2 != parity:
+                    lex += 1
+                    x[3] += 1
+                a = oracle.su3_staple(ext, links, x, mu)
+                fo = oracle.lp_features(a, 6.0)
+                assert np.abs(f[t] - fo).max() <= 2e-5 * max(1.0, np.abs(fo).max())
+                mo = links[4 * lex + mu] @ a
+                mo18 = np.stack([mo.real, mo.imag], -1).reshape(18)
+                assert np.abs(m[t] - mo18).max() <= 2e-5 * 6
+
+
+def test_gradient_matches_oracle(oracle):
+    import ymgpu
+    with thermal_f32([4, 4, 4, 6], 1) as ens, ymgpu.ProposalModel(seed=5, initial_scale=0.5) as model:
+        f, m, b = ymgpu.learned.records(ens, 0, 1)
+        n = 300                                    # not a multiple of the 128-row tile
+        p = model.params
+        obj, g = model.gradient(f[:n], m[:n], b[:n])
+        obj_o, g_o = oracle.lp_loss_grad(p, f[:n], m[:n], b[:n])
+    assert abs(obj - obj_o) <= 1e-4 * abs(obj_o)
+    assert np.linalg.norm(g - g_o) <= 0.03 * np.linalg.norm(g_o), np.linalg.norm(g - g_o) / np.linalg.norm(g_o)
+    for name, lo, hi in (("W1", 0, 1024), ("b1", 1024, 1088), ("W2", 1088, 5184), ("b2", 5184, 5248),
+                         ("W3", 5248, 5248 + 576), ("b3", 6272, 6281)):
+        d = np.linalg.norm(g[lo:hi] - g_o[lo:hi])
+        assert d <= 0.05 * np.linalg.norm(g_o[lo:hi]) + 1e-7, name
+    assert not np.any(g[5248 + 576:6272]) and not np.any(g[6281:])
+
+
+def test_learned_sweep_matches_oracle(oracle):
+    import ymgpu
+    ext = [4, 4, 4, 4]
+    with thermal_f32(ext, 1, sweeps=40) as ens, ymgpu.ProposalModel(seed=3, initial_scale=0.7) as model:
+        links = ens.download(0)
+        sweep = ens.sweep_index
+        p0, a0 = ens.accounting()
+        model.sweeps(ens, 1)
+        p1, a1 = ens.accounting()
+        dev = ens.download(0)
+        plaq_dev = ens.average_plaquette()[0]
+        npr, nac = oracle.lp_cb_sweep(ext, links, 6.0, model.params, int(ens.seeds[0]), sweep)
+    assert int(p1[0] - p0[0]) == npr == 8 * 4 * 256
+    assert abs(int(a1[0] - a0[0]) - nac) <= 0.01 * npr
+    plaq_or = oracle.su3_average_plaquette(ext, links)
+    assert abs(plaq_dev - plaq_or) <= 2e-3
+    # most links agree to binary32 accuracy (a borderline decision may diverge)
+    close = np.abs(dev - links).reshape(len(links), -1).max(1) <= 1e-4
+    assert close.mean() >= 0.97
+
+
+def test_training_raises_objective():
+    import ymgpu
+    with thermal_f32([4, 4, 4, 4], 16) as ens, ymgpu.ProposalModel(seed=11) as model:
+        hist = model.train(ens, 240, sweeps_per_step=1, plain_angle=0.3, lr=3e-3)
+        f, _, _ = ymgpu.learned.records(ens, 0, 0)
+        _, s = ymgpu.learned.proposal(model.forward(f))
+    assert np.all(np.isfinite(hist))
+    assert hist[-40:].mean() > 1.5 * hist[:8].mean()
+    assert s.mean() > 0.45           # started at 0.3
+
+
+def test_trained_proposal_beats_plain():
+    """Plaquette autocorrelation per sweep: the trained proposal against
+    plain Metropolis with uniform generators at half width 0.3, same
+    lattices, same plaquette within errors."""
+    import ymgpu
+    from ymgpu.su2_ensemble import diagnostics
+    nch, meas = 32, 1500
+    with thermal_f32([8, 8, 8, 8], nch, sweeps=300) as ens, ymgpu.ProposalModel(seed=13) as model:
+        model.train(ens, 400, sweeps_per_step=1, plain_angle=0.3, lr=3e-3)
+        plain = ens.like()
+        ens.copy_to(plain)
+        model.sweeps(ens, 200)
+        plain.metropolis_sweeps(0.3, 200, "uniform")
+        s_l = model.measured_sweeps(ens, meas)
+        s_p = plain.measured_sweeps(0.3, meas, 1, "uniform")
+        plain.close()
+    tau = lambda s: np.mean([diagnostics(s[:, c], 200)[0].integrated_autocorrelation_time
+                             for c in range(nch)])
+    t_l, t_p = tau(s_l), tau(s_p)
+    m_l, m_p = s_l.mean(0), s_p.mean(0)
+    err = np.hypot(m_l.std(ddof=1), m_p.std(ddof=1)) / np.sqrt(nch)
+    assert abs(m_l.mean() - m_p.mean()) <= 4 * err, (m_l.mean(), m_p.mean(), err)
+    assert t_l < t_p / 1.5, (t_l, t_p)

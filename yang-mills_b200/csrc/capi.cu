@@ -911,3 +911,362 @@ int32_t ym_profile_read(ym_ensemble *e, int32_t kernel, double *total_ms, int64_
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------ learned proposal
+namespace {
+
+void free_model(ym_proposal_model *m) {
+    void *ptrs[] = {m->d_params, m->d_adam_m, m->d_adam_v, m->d_image, m->d_error, m->d_feat,
+                    m->d_mrec, m->d_b3, m->d_y, m->d_partial, m->d_grad, m->d_objective};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    if (m->stream) cudaStreamDestroy(m->stream);
+}
+
+int32_t model_device(const ym_proposal_model *m) { return cuda_status(cudaSetDevice(m->device)); }
+
+cudaError_t ensure_rows(ym_proposal_model *m, int64_t rows) {
+    rows = (rows + 127) / 128 * 128;
+    if (rows <= m->row_capacity) return cudaSuccess;
+    float **bufs[] = {&m->d_feat, &m->d_mrec, &m->d_b3, &m->d_y};
+    for (float **b : bufs)
+        if (*b) {
+            cudaFree(*b);
+            *b = nullptr;
+        }
+    m->row_capacity = 0;
+    cudaError_t err = dalloc(&m->d_feat, (size_t)rows * 16);
+    if (err == cudaSuccess) err = dalloc(&m->d_mrec, (size_t)rows * 18);
+    if (err == cudaSuccess) err = dalloc(&m->d_b3, (size_t)rows);
+    if (err == cudaSuccess) err = dalloc(&m->d_y, (size_t)rows * 16);
+    if (err == cudaSuccess) m->row_capacity = rows;
+    return err;
+}
+
+cudaError_t ensure_partials(ym_proposal_model *m, int64_t tiles) {
+    if (tiles <= m->partial_capacity) return cudaSuccess;
+    if (m->d_partial) cudaFree(m->d_partial);
+    m->d_partial = nullptr;
+    m->partial_capacity = 0;
+    cudaError_t err = dalloc(&m->d_partial, (size_t)(tiles * ym::kLpPartialStride));
+    if (err == cudaSuccess) m->partial_capacity = tiles;
+    return err;
+}
+
+cudaError_t ensure_objectives(ym_proposal_model *m, int64_t n) {
+    if (n <= m->objective_capacity) return cudaSuccess;
+    if (m->d_objective) cudaFree(m->d_objective);
+    m->d_objective = nullptr;
+    m->objective_capacity = 0;
+    cudaError_t err = dalloc(&m->d_objective, (size_t)n);
+    if (err == cudaSuccess) m->objective_capacity = n;
+    return err;
+}
+
+// Outputs 9..15 are padding: their weights and biases stay zero.
+void zero_padding(float *p) {
+    for (int i = YM_LP_OFF_W3 + 9 * 64; i < YM_LP_OFF_B3; ++i) p[i] = 0.0f;
+    for (int i = YM_LP_OFF_B3 + 9; i < YM_LP_PARAMS; ++i) p[i] = 0.0f;
+}
+
+int32_t upload_params(ym_proposal_model *m, const float *host) {
+    std::vector<float> p(host, host + YM_LP_PARAMS);
+    zero_padding(p.data());
+    for (float v : p)
+        if (!std::isfinite(v)) return YM_ERR_INVALID_ARGUMENT;
+    YM_CUDA(cudaMemcpyAsync(m->d_params, p.data(), sizeof(float) * YM_LP_PARAMS, cudaMemcpyHostToDevice,
+                            m->stream));
+    YM_CUDA(cudaMemsetAsync(m->d_adam_m, 0, sizeof(float) * YM_LP_PARAMS, m->stream));
+    YM_CUDA(cudaMemsetAsync(m->d_adam_v, 0, sizeof(float) * YM_LP_PARAMS, m->stream));
+    YM_CUDA(cudaMemsetAsync(m->d_image, 0, 12288, m->stream));
+    YM_CUDA(ym::launch_lp_image(m, m->stream));
+    YM_CUDA(cudaStreamSynchronize(m->stream));
+    m->adam_step = 0;
+    return YM_OK;
+}
+
+// Reads and clears the model's device error bits after `st` drains.
+int32_t take_model_error(ym_proposal_model *m, cudaStream_t st) {
+    unsigned bits = 0;
+    YM_CUDA(cudaMemcpyAsync(&bits, m->d_error, sizeof bits, cudaMemcpyDeviceToHost, st));
+    YM_CUDA(cudaStreamSynchronize(st));
+    if (!bits) return YM_OK;
+    YM_CUDA(cudaMemsetAsync(m->d_error, 0, sizeof(unsigned), st));
+    YM_CUDA(cudaStreamSynchronize(st));
+    return YM_ERR_DEVICE_WAIT_TIMEOUT;
+}
+
+int32_t require_learned(const ym_ensemble *e, const ym_proposal_model *m) {
+    if (e->group != YM_GROUP_SU3) return YM_ERR_WRONG_GROUP;
+    if (e->precision != YM_PREC_F32_TWO_ROW) return YM_ERR_UNSUPPORTED_PRECISION;
+    int32_t st = validate_su3_betas(e);
+    if (st) return st;
+    st = require_checkerboard(e);
+    if (st) return st;
+    if (m && m->device != e->device) return YM_ERR_INVALID_ARGUMENT;
+    return YM_OK;
+}
+
+cudaError_t plain_uniform_sweep(ym_ensemble *e, double angle) {
+    for (int parity = 0; parity < 2; ++parity)
+        for (int mu = 0; mu < 4; ++mu) {
+            cudaError_t err = ym::launch_f32_metropolis(e, parity, mu, angle, YM_GEN_UNIFORM);
+            if (err != cudaSuccess) return err;
+        }
+    cudaError_t err = ym::launch_f32_reunitarize(e);
+    return err == cudaSuccess ? ym::launch_advance_sweep(e) : err;
+}
+
+cudaError_t learned_sweep(ym_ensemble *e, ym_proposal_model *m) {
+    for (int parity = 0; parity < 2; ++parity)
+        for (int mu = 0; mu < 4; ++mu) {
+            cudaError_t err = timed(e, YM_KERNEL_LEARNED, [&] { return ym::launch_lp_sweep(e, m, parity, mu); });
+            if (err != cudaSuccess) return err;
+        }
+    cudaError_t err = timed(e, YM_KERNEL_AUX, [&] { return ym::launch_f32_reunitarize(e); });
+    return err == cudaSuccess ? ym::launch_advance_sweep(e) : err;
+}
+
+int64_t half_sites(const ym_ensemble *e) {
+    int64_t n = 0;
+    for (const ChainInfo &c : e->chains) n += c.half;
+    return n;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t ym_model_create(int32_t device, uint64_t seed, double initial_scale, ym_proposal_model **out) {
+    if (!out) return YM_ERR_NULL_ARGUMENT;
+    *out = nullptr;
+    if (!std::isfinite(initial_scale) || initial_scale <= YM_LP_SCALE_MIN || initial_scale >= YM_LP_SCALE_MAX)
+        return YM_ERR_INVALID_ARGUMENT;
+    ym_proposal_model *m = new (std::nothrow) ym_proposal_model();
+    if (!m) return YM_ERR_CUDA;
+    m->device = device;
+    auto fail = [&](int32_t st) {
+        free_model(m);
+        delete m;
+        return st;
+    };
+    if (cudaSetDevice(device) != cudaSuccess) return fail(cuda_status(cudaSetDevice(device)));
+    cudaError_t err = cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking);
+    if (err == cudaSuccess) err = dalloc(&m->d_params, YM_LP_PARAMS);
+    if (err == cudaSuccess) err = dalloc(&m->d_adam_m, YM_LP_PARAMS);
+    if (err == cudaSuccess) err = dalloc(&m->d_adam_v, YM_LP_PARAMS);
+    if (err == cudaSuccess) err = dalloc(&m->d_grad, YM_LP_PARAMS);
+    if (err == cudaSuccess) err = dalloc(&m->d_image, 12288);
+    if (err == cudaSuccess) err = dalloc(&m->d_error, 1);
+    if (err == cudaSuccess) err = cudaMemset(m->d_error, 0, sizeof(unsigned));
+    if (err != cudaSuccess) return fail(cuda_status(err));
+    // He-uniform draw from a SplitMix64 stream of the seed; the last layer
+    // scaled by 1/8; zero biases except the scale output.
+    std::vector<float> p(YM_LP_PARAMS, 0.0f);
+    uint64_t n = 0;
+    auto uniform = [&](double bound) {
+        const double u = (double)(ym_splitmix64_at(seed, n++) >> 11) * (1.0 / 9007199254740992.0);
+        return (float)((2.0 * u - 1.0) * bound);
+    };
+    for (int i = 0; i < 64 * 16; ++i) p[YM_LP_OFF_W1 + i] = uniform(std::sqrt(6.0 / 16.0));
+    for (int i = 0; i < 64 * 64; ++i) p[YM_LP_OFF_W2 + i] = uniform(std::sqrt(6.0 / 64.0));
+    for (int i = 0; i < 9 * 64; ++i) p[YM_LP_OFF_W3 + i] = uniform(std::sqrt(6.0 / 64.0) / 8.0);
+    const double q = (initial_scale - YM_LP_SCALE_MIN) / (YM_LP_SCALE_MAX - YM_LP_SCALE_MIN);
+    p[YM_LP_OFF_B3 + 8] = (float)std::log(q / (1.0 - q));
+    const int32_t st = upload_params(m, p.data());
+    if (st) return fail(st);
+    *out = m;
+    return YM_OK;
+}
+
+int32_t ym_model_destroy(ym_proposal_model *m) {
+    if (!m) return YM_ERR_NULL_ARGUMENT;
+    cudaSetDevice(m->device);
+    if (m->stream) cudaStreamSynchronize(m->stream);
+    free_model(m);
+    delete m;
+    return YM_OK;
+}
+
+int32_t ym_model_get_params(ym_proposal_model *m, float *params) {
+    if (!m || !params) return YM_ERR_NULL_ARGUMENT;
+    int32_t st = model_device(m);
+    if (st) return st;
+    YM_CUDA(cudaMemcpyAsync(params, m->d_params, sizeof(float) * YM_LP_PARAMS, cudaMemcpyDeviceToHost,
+                            m->stream));
+    YM_CUDA(cudaStreamSynchronize(m->stream));
+    return YM_OK;
+}
+
+int32_t ym_model_set_params(ym_proposal_model *m, const float *params) {
+    if (!m || !params) return YM_ERR_NULL_ARGUMENT;
+    int32_t st = model_device(m);
+    if (st) return st;
+    return upload_params(m, params);
+}
+
+int32_t ym_model_forward(ym_proposal_model *m, const float *features, int64_t n, float *outputs) {
+    if (!m || ((!features || !outputs) && n > 0)) return YM_ERR_NULL_ARGUMENT;
+    if (n < 0) return YM_ERR_INVALID_ARGUMENT;
+    if (n == 0) return YM_OK;
+    int32_t st = model_device(m);
+    if (st) return st;
+    YM_CUDA(ensure_rows(m, n));
+    YM_CUDA(cudaMemcpyAsync(m->d_feat, features, sizeof(float) * 16 * (size_t)n, cudaMemcpyHostToDevice,
+                            m->stream));
+    YM_CUDA(ym::launch_lp_forward(m, m->d_feat, n, m->d_y, m->stream));
+    YM_CUDA(cudaMemcpyAsync(outputs, m->d_y, sizeof(float) * 16 * (size_t)n, cudaMemcpyDeviceToHost,
+                            m->stream));
+    return take_model_error(m, m->stream);
+}
+
+int32_t ym_model_gradient(ym_proposal_model *m, const float *features, const float *mrec,
+                          const double *beta, int64_t n, double *objective, float *grad) {
+    if (!m || !features || !mrec || !beta || !objective || !grad) return YM_ERR_NULL_ARGUMENT;
+    if (n <= 0) return YM_ERR_INVALID_ARGUMENT;
+    std::vector<float> b3((size_t)n);
+    for (int64_t i = 0; i < n; ++i) {
+        if (!std::isfinite(beta[i]) || beta[i] < 0.0 || beta[i] > kMaxSu3Beta)
+            return YM_ERR_BETA_OUTSIDE_REFERENCE_RANGE;
+        b3[(size_t)i] = (float)(beta[i] / 3.0);
+    }
+    int32_t st = model_device(m);
+    if (st) return st;
+    const int64_t tiles = (n + 127) / 128;
+    YM_CUDA(ensure_rows(m, n));
+    YM_CUDA(ensure_partials(m, tiles));
+    YM_CUDA(ensure_objectives(m, 1));
+    YM_CUDA(cudaMemcpyAsync(m->d_feat, features, sizeof(float) * 16 * (size_t)n, cudaMemcpyHostToDevice, m->stream));
+    YM_CUDA(cudaMemcpyAsync(m->d_mrec, mrec, sizeof(float) * 18 * (size_t)n, cudaMemcpyHostToDevice, m->stream));
+    YM_CUDA(cudaMemcpyAsync(m->d_b3, b3.data(), sizeof(float) * (size_t)n, cudaMemcpyHostToDevice, m->stream));
+    YM_CUDA(ym::launch_lp_grad(m, m->d_feat, m->d_mrec, m->d_b3, n, m->stream));
+    YM_CUDA(ym::launch_lp_adam(m, tiles, n, 0.0f, 0, m->d_grad, m->d_objective, m->stream));
+    YM_CUDA(cudaMemcpyAsync(grad, m->d_grad, sizeof(float) * YM_LP_PARAMS, cudaMemcpyDeviceToHost, m->stream));
+    YM_CUDA(cudaMemcpyAsync(objective, m->d_objective, sizeof(double), cudaMemcpyDeviceToHost, m->stream));
+    return take_model_error(m, m->stream);
+}
+
+int32_t ym_learned_records(ym_ensemble *e, int32_t parity, int32_t mu, float *features, float *mrec,
+                           double *beta, int64_t *n_out) {
+    if (!e || !n_out) return YM_ERR_NULL_ARGUMENT;
+    int32_t st = require_learned(e, nullptr);
+    if (st) return st;
+    if (parity < 0 || parity > 1 || mu < 0 || mu > 3) return YM_ERR_INVALID_ARGUMENT;
+    *n_out = half_sites(e);
+    if (!features || !mrec || !beta) return YM_OK;
+    st = set_device(e);
+    if (st) return st;
+    const int64_t rows = e->n_half_tiles * 128;
+    float *d_f = nullptr, *d_m = nullptr, *d_b = nullptr;
+    cudaError_t err = dalloc(&d_f, (size_t)rows * 16);
+    if (err == cudaSuccess) err = dalloc(&d_m, (size_t)rows * 18);
+    if (err == cudaSuccess) err = dalloc(&d_b, (size_t)rows);
+    std::vector<float> hf, hm;
+    if (err == cudaSuccess) err = ym::launch_lp_records(e, parity, mu, d_f, d_m, d_b);
+    if (err == cudaSuccess) {
+        hf.resize((size_t)rows * 16);
+        hm.resize((size_t)rows * 18);
+        err = cudaMemcpyAsync(hf.data(), d_f, hf.size() * sizeof(float), cudaMemcpyDeviceToHost, e->stream);
+    }
+    if (err == cudaSuccess)
+        err = cudaMemcpyAsync(hm.data(), d_m, hm.size() * sizeof(float), cudaMemcpyDeviceToHost, e->stream);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);
+    cudaFree(d_f);
+    cudaFree(d_m);
+    cudaFree(d_b);
+    YM_CUDA(err);
+    // tiles are laid out chain by chain, 128 sites of the parity each
+    int64_t tile0 = 0, out = 0;
+    for (const ChainInfo &c : e->chains) {
+        for (int64_t t = 0; t < c.half; ++t, ++out) {
+            const int64_t row = tile0 * 128 + t;
+            std::memcpy(features + out * 16, hf.data() + row * 16, 16 * sizeof(float));
+            std::memcpy(mrec + out * 18, hm.data() + row * 18, 18 * sizeof(float));
+            beta[out] = c.beta;
+        }
+        tile0 += (c.half + 127) / 128;
+    }
+    return YM_OK;
+}
+
+int32_t ym_model_train(ym_proposal_model *m, ym_ensemble *e, int64_t n_steps, int64_t sweeps_per_step,
+                       double plain_angle, double lr, double *objective_history) {
+    if (!m || !e) return YM_ERR_NULL_ARGUMENT;
+    int32_t st = require_learned(e, m);
+    if (st) return st;
+    st = validate_angle(plain_angle);
+    if (st) return st;
+    if (n_steps < 0 || sweeps_per_step < 0 || !std::isfinite(lr) || lr <= 0.0) return YM_ERR_INVALID_ARGUMENT;
+    if (n_steps == 0) return YM_OK;
+    st = set_device(e);
+    if (st) return st;
+    const int64_t rows = e->n_half_tiles * 128;
+    YM_CUDA(ensure_rows(m, rows));
+    YM_CUDA(ensure_partials(m, e->n_half_tiles));
+    YM_CUDA(ensure_objectives(m, n_steps));
+    YM_CUDA(cudaStreamSynchronize(m->stream));   // model-stream work before ensemble-stream work
+    const int64_t n_valid = half_sites(e);
+    for (int64_t step = 0; step < n_steps; ++step) {
+        for (int64_t k = 0; k < sweeps_per_step; ++k) YM_CUDA(plain_uniform_sweep(e, plain_angle));
+        const int sub = (int)(step % 8);
+        YM_CUDA(ym::launch_lp_records(e, sub / 4, sub % 4, m->d_feat, m->d_mrec, m->d_b3));
+        YM_CUDA(ym::launch_lp_grad(m, m->d_feat, m->d_mrec, m->d_b3, rows, e->stream));
+        YM_CUDA(ym::launch_lp_adam(m, e->n_half_tiles, n_valid, (float)lr, 1, nullptr,
+                                   m->d_objective + step, e->stream));
+    }
+    if (objective_history)
+        YM_CUDA(cudaMemcpyAsync(objective_history, m->d_objective, sizeof(double) * (size_t)n_steps,
+                                cudaMemcpyDeviceToHost, e->stream));
+    for (int64_t ch = 0; ch < e->n_chains; ++ch)
+        e->proposals[ch] += (uint64_t)(n_steps * sweeps_per_step) * 32u * (uint64_t)e->chains[ch].volume;
+    return take_model_error(m, e->stream);
+}
+
+int32_t ym_su3_learned_sweeps(ym_ensemble *e, ym_proposal_model *m, int64_t n_sweeps) {
+    if (!e || !m) return YM_ERR_NULL_ARGUMENT;
+    int32_t st = require_learned(e, m);
+    if (st) return st;
+    if (n_sweeps < 0) return YM_ERR_INVALID_ARGUMENT;
+    st = set_device(e);
+    if (st) return st;
+    YM_CUDA(cudaStreamSynchronize(m->stream));
+    for (int64_t k = 0; k < n_sweeps; ++k) YM_CUDA(learned_sweep(e, m));
+    for (int64_t ch = 0; ch < e->n_chains; ++ch)
+        e->proposals[ch] += (uint64_t)n_sweeps * 32u * (uint64_t)e->chains[ch].volume;
+    return take_model_error(m, e->stream);
+}
+
+int32_t ym_su3_learned_measured_sweeps(ym_ensemble *e, ym_proposal_model *m, int64_t n_measurements,
+                                       int64_t sweeps_per_measurement, double *series) {
+    if (!e || !m || (!series && n_measurements > 0)) return YM_ERR_NULL_ARGUMENT;
+    int32_t st = require_learned(e, m);
+    if (st) return st;
+    if (n_measurements < 0 || sweeps_per_measurement < 0) return YM_ERR_INVALID_ARGUMENT;
+    if (n_measurements == 0) return YM_OK;
+    st = set_device(e);
+    if (st) return st;
+    YM_CUDA(cudaStreamSynchronize(m->stream));
+    if (e->series_capacity < n_measurements) {
+        if (e->d_series) cudaFree(e->d_series);
+        e->d_series = nullptr;
+        e->series_capacity = 0;
+        YM_CUDA(dalloc(&e->d_series, (size_t)(n_measurements * e->n_chains)));
+        e->series_capacity = n_measurements;
+    }
+    if (!e->d_series_row) YM_CUDA(dalloc(&e->d_series_row, 1));
+    YM_CUDA(cudaMemsetAsync(e->d_series_row, 0, sizeof(uint64_t), e->stream));
+    for (int64_t meas = 0; meas < n_measurements; ++meas) {
+        for (int64_t k = 0; k < sweeps_per_measurement; ++k) YM_CUDA(learned_sweep(e, m));
+        YM_CUDA(ym::launch_f32_plaquette_partials(e));
+        YM_CUDA(ym::launch_chain_reduce(e, e->d_partial, e->d_result, 0, 6.0));
+        YM_CUDA(ym::launch_store_series(e, e->d_series, e->d_series_row));
+    }
+    YM_CUDA(cudaMemcpyAsync(series, e->d_series, (size_t)(n_measurements * e->n_chains) * sizeof(double),
+                            cudaMemcpyDeviceToHost, e->stream));
+    for (int64_t ch = 0; ch < e->n_chains; ++ch)
+        e->proposals[ch] += (uint64_t)(n_measurements * sweeps_per_measurement) * 32u *
+                            (uint64_t)e->chains[ch].volume;
+    return take_model_error(m, e->stream);
+}
+
+}  // extern "C"

@@ -16,6 +16,7 @@
 // (Gram-Schmidt on rows 0-1) and rounds back once per sweep.
 #include <cuda_runtime.h>
 
+#include "su3_f32.cuh"
 #include "su3_haar.cuh"
 #include "ym_internal.hpp"
 
@@ -24,260 +25,7 @@ namespace ym {
 namespace {
 
 constexpr int T = kSweepThreads;
-
-struct cf {
-    float re, im;
-};
-
-__device__ __forceinline__ cf cfm(float r, float i) { return cf{r, i}; }
-__device__ __forceinline__ cf cfadd(cf a, cf b) { return cf{a.re + b.re, a.im + b.im}; }
-__device__ __forceinline__ cf cfsub(cf a, cf b) { return cf{a.re - b.re, a.im - b.im}; }
-__device__ __forceinline__ cf cfmul(cf a, cf b) {
-    return cf{fmaf(a.re, b.re, -a.im * b.im), fmaf(a.re, b.im, a.im * b.re)};
-}
-__device__ __forceinline__ cf cfconj(cf a) { return cf{a.re, -a.im}; }
-// acc += a * b
-__device__ __forceinline__ void cffma(cf &acc, cf a, cf b) {
-    acc.re = fmaf(a.re, b.re, acc.re);
-    acc.re = fmaf(-a.im, b.im, acc.re);
-    acc.im = fmaf(a.re, b.im, acc.im);
-    acc.im = fmaf(a.im, b.re, acc.im);
-}
-
-struct m3f {
-    cf e[3][3];
-};
-
-__device__ __forceinline__ void third_row(m3f &u) {
-    u.e[2][0] = cfconj(cfsub(cfmul(u.e[0][1], u.e[1][2]), cfmul(u.e[0][2], u.e[1][1])));
-    u.e[2][1] = cfconj(cfsub(cfmul(u.e[0][2], u.e[1][0]), cfmul(u.e[0][0], u.e[1][2])));
-    u.e[2][2] = cfconj(cfsub(cfmul(u.e[0][0], u.e[1][1]), cfmul(u.e[0][1], u.e[1][0])));
-}
-
-__device__ __forceinline__ m3f load_f(const float2 *__restrict__ links, const ChainInfo &c, int64_t s,
-                                      int mu) {
-    const float2 *p = links + c.offset + (int64_t)(mu * 6) * c.volume + s;
-    m3f u;
-#pragma unroll
-    for (int e = 0; e < 6; ++e) {
-        const float2 v = __ldg(p + (int64_t)e * c.volume);
-        u.e[e / 3][e % 3] = cfm(v.x, v.y);
-    }
-    third_row(u);
-    return u;
-}
-
-__device__ __forceinline__ void store_f(float2 *links, const ChainInfo &c, int64_t s, int mu,
-                                        const m3f &u) {
-    float2 *p = links + c.offset + (int64_t)(mu * 6) * c.volume + s;
-#pragma unroll
-    for (int e = 0; e < 6; ++e) p[(int64_t)e * c.volume] = make_float2(u.e[e / 3][e % 3].re, u.e[e / 3][e % 3].im);
-}
-
-// Two stored rows -> a binary64 matrix with the third row rebuilt in binary64.
-__device__ __forceinline__ m3 load_as_f64(const float2 *__restrict__ links, const ChainInfo &c,
-                                          int64_t s, int mu) {
-    const float2 *p = links + c.offset + (int64_t)(mu * 6) * c.volume + s;
-    m3 u;
-#pragma unroll
-    for (int e = 0; e < 6; ++e) {
-        const float2 v = __ldg(p + (int64_t)e * c.volume);
-        u.e[e / 3][e % 3] = cmake((double)v.x, (double)v.y);
-    }
-    u.e[2][0] = cconj(csub(cmul(u.e[0][1], u.e[1][2]), cmul(u.e[0][2], u.e[1][1])));
-    u.e[2][1] = cconj(csub(cmul(u.e[0][2], u.e[1][0]), cmul(u.e[0][0], u.e[1][2])));
-    u.e[2][2] = cconj(csub(cmul(u.e[0][0], u.e[1][1]), cmul(u.e[0][1], u.e[1][0])));
-    return u;
-}
-
-__device__ __forceinline__ void store_rows_from_f64(float2 *links, const ChainInfo &c, int64_t s,
-                                                    int mu, const m3 &u) {
-    float2 *p = links + c.offset + (int64_t)(mu * 6) * c.volume + s;
-#pragma unroll
-    for (int e = 0; e < 6; ++e)
-        p[(int64_t)e * c.volume] = make_float2((float)u.e[e / 3][e % 3].re, (float)u.e[e / 3][e % 3].im);
-}
-
-__device__ __forceinline__ m3f lkf(const float2 *links, const ChainInfo &c, const Nb &n, int mu) {
-    return load_f(links, c, storage_index(c, n.lex, n.par), mu);
-}
-
-// Staple sum in binary32: same terms and order as the FP64 path.
-template <int MU>
-__device__ __forceinline__ m3f staple_f(const float2 *__restrict__ links, const ChainInfo &c,
-                                        const Coord &x, int par) {
-    m3f a;
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j) a.e[i][j] = cfm(0.f, 0.f);
-    const Nb self{x.lex, par};
-    const Nb pm = step(c, x.x, x.lex, par, MU, +1);
-#pragma unroll
-    for (int nu = 0; nu < 4; ++nu) {
-        if (nu == MU) continue;
-        const Nb pn = step(c, x.x, x.lex, par, nu, +1);
-        const Nb mn = step(c, x.x, x.lex, par, nu, -1);
-        const Nb mnpm = step(c, x.x, mn.lex, mn.par, MU, +1);
-        {
-            const m3f l2 = lkf(links, c, pn, MU);
-            const m3f l1 = lkf(links, c, pm, nu);
-            m3f p;
-#pragma unroll
-            for (int r = 0; r < 3; ++r)
-#pragma unroll
-                for (int k = 0; k < 3; ++k) {
-                    cf v = cfm(0.f, 0.f);
-#pragma unroll
-                    for (int j = 0; j < 3; ++j) cffma(v, l1.e[r][j], cfconj(l2.e[k][j]));
-                    p.e[r][k] = v;
-                }
-            const m3f l3 = lkf(links, c, self, nu);
-#pragma unroll
-            for (int r = 0; r < 3; ++r)
-#pragma unroll
-                for (int col = 0; col < 3; ++col)
-#pragma unroll
-                    for (int k = 0; k < 3; ++k) cffma(a.e[r][col], p.e[r][k], cfconj(l3.e[col][k]));
-        }
-        {
-            const m3f l2 = lkf(links, c, mn, MU);
-            const m3f l1 = lkf(links, c, mnpm, nu);
-            m3f p;
-#pragma unroll
-            for (int r = 0; r < 3; ++r)
-#pragma unroll
-                for (int k = 0; k < 3; ++k) {
-                    cf v = cfm(0.f, 0.f);
-#pragma unroll
-                    for (int j = 0; j < 3; ++j) cffma(v, cfconj(l1.e[j][r]), cfconj(l2.e[k][j]));
-                    p.e[r][k] = v;
-                }
-            const m3f l3 = lkf(links, c, mn, nu);
-#pragma unroll
-            for (int r = 0; r < 3; ++r)
-#pragma unroll
-                for (int col = 0; col < 3; ++col)
-#pragma unroll
-                    for (int k = 0; k < 3; ++k) cffma(a.e[r][col], p.e[r][k], l3.e[k][col]);
-        }
-    }
-    return a;
-}
-
-// Row i of Re Tr(X A) in binary64 from binary32 operands.
-__device__ __forceinline__ double retr_row64(const cf *xrow, const m3f &a, int i) {
-    double acc = (double)xrow[0].re * (double)a.e[0][i].re;
-    acc = fma(-(double)xrow[0].im, (double)a.e[0][i].im, acc);
-    acc = fma((double)xrow[1].re, (double)a.e[1][i].re, acc);
-    acc = fma(-(double)xrow[1].im, (double)a.e[1][i].im, acc);
-    acc = fma((double)xrow[2].re, (double)a.e[2][i].re, acc);
-    acc = fma(-(double)xrow[2].im, (double)a.e[2][i].im, acc);
-    return acc;
-}
-
-__device__ __forceinline__ bool accept64(double old_tr, double new_tr, double beta3, double unif) {
-    const double m = fmax(beta3 * (old_tr - new_tr), 0.0);
-    return (m == 0.0) ? true : (unif < exp(-m));
-}
-
-template <int I0, int I1>
-__device__ __forceinline__ void hit_block_f(m3f &u, const m3f &a, double rr[3], double &old_tr,
-                                            int kind, float c, float s, double beta3, double unif,
-                                            unsigned &accepted) {
-    cf n0[3], n1[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        const float x0 = u.e[I0][k].re, y0 = u.e[I0][k].im;
-        const float x1 = u.e[I1][k].re, y1 = u.e[I1][k].im;
-        if (kind == 0) {
-            n0[k] = cfm(fmaf(c, x0, -s * y1), fmaf(c, y0, s * x1));
-            n1[k] = cfm(fmaf(c, x1, -s * y0), fmaf(s, x0, c * y1));
-        } else if (kind == 1) {
-            n0[k] = cfm(fmaf(c, x0, s * x1), fmaf(c, y0, s * y1));
-            n1[k] = cfm(fmaf(c, x1, -s * x0), fmaf(c, y1, -s * y0));
-        } else {
-            n0[k] = cfm(fmaf(c, x0, -s * y0), fmaf(c, y0, s * x0));
-            n1[k] = cfm(fmaf(c, x1, s * y1), fmaf(c, y1, -s * x1));
-        }
-    }
-    double q[3] = {rr[0], rr[1], rr[2]};
-    q[I0] = retr_row64(n0, a, I0);
-    q[I1] = retr_row64(n1, a, I1);
-    const double new_tr = (q[0] + q[1]) + q[2];
-    if (accept64(old_tr, new_tr, beta3, unif)) {
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            u.e[I0][k] = n0[k];
-            u.e[I1][k] = n1[k];
-        }
-        rr[I0] = q[I0];
-        rr[I1] = q[I1];
-        old_tr = new_tr;
-        accepted++;
-    }
-}
-
-__device__ __forceinline__ void hit_diag_f(m3f &u, const m3f &a, double rr[3], double &old_tr,
-                                           cf e1, cf e2, double beta3, double unif,
-                                           unsigned &accepted) {
-    cf n[3][3];
-    double q[3];
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-        const cf e = i < 2 ? e1 : e2;
-#pragma unroll
-        for (int k = 0; k < 3; ++k) n[i][k] = cfmul(e, u.e[i][k]);
-        q[i] = retr_row64(n[i], a, i);
-    }
-    const double new_tr = (q[0] + q[1]) + q[2];
-    if (accept64(old_tr, new_tr, beta3, unif)) {
-#pragma unroll
-        for (int i = 0; i < 3; ++i) {
-#pragma unroll
-            for (int k = 0; k < 3; ++k) u.e[i][k] = n[i][k];
-            rr[i] = q[i];
-        }
-        old_tr = new_tr;
-        accepted++;
-    }
-}
-
-// exp(i theta T^a) in closed form: c = cos(theta/2), s = sin(theta/2) for
-// the SU(2) subgroups; diag(e^{i theta/(2 sqrt3)} x2, e^{-i theta/sqrt3}).
-__device__ __forceinline__ unsigned visit_f(m3f &u, const m3f &a, double beta3, double angle,
-                                            uint64_t key, int uniform) {
-    double rr[3];
-#pragma unroll
-    for (int i = 0; i < 3; ++i) rr[i] = retr_row64(u.e[i], a, i);
-    double old_tr = (rr[0] + rr[1]) + rr[2];
-    unsigned accepted = 0;
-#pragma unroll 1
-    for (int h = 0; h < 8; ++h) {
-        const uint64_t w_angle = splitmix_at(key, (uint64_t)(2 * h));
-        const uint64_t w_acc = splitmix_at(key, (uint64_t)(2 * h + 1));
-        const int g = uniform ? (int)((w_angle >> 52) & 7) : h;
-        const float theta = (float)grid_angle(w_angle, angle);
-        const double unif = unit_from(w_acc);
-        if (g == 7) {
-            float s1, c1, s2, c2;
-            sincosf(theta * 0.28867513459481287f, &s1, &c1);
-            sincosf(theta * -0.57735026918962573f, &s2, &c2);
-            hit_diag_f(u, a, rr, old_tr, cfm(c1, s1), cfm(c2, s2), beta3, unif, accepted);
-        } else {
-            float s, c;
-            sincosf(0.5f * theta, &s, &c);
-            const int kind = (g == 2) ? 2 : ((g == 1 || g == 4 || g == 6) ? 1 : 0);
-            if (g <= 2)
-                hit_block_f<0, 1>(u, a, rr, old_tr, kind, c, s, beta3, unif, accepted);
-            else if (g <= 4)
-                hit_block_f<0, 2>(u, a, rr, old_tr, kind, c, s, beta3, unif, accepted);
-            else
-                hit_block_f<1, 2>(u, a, rr, old_tr, kind, c, s, beta3, unif, accepted);
-        }
-    }
-    return accepted;
-}
+using namespace f32;
 
 template <int MU>
 __global__ void __launch_bounds__(T)

@@ -14,6 +14,7 @@ namespace ym {
 
 constexpr int kSweepThreads = 128;   // threads per tile of a sub-sweep
 constexpr int kSiteThreads = 128;    // threads per tile of a measurement
+constexpr int64_t kLpPartialStride = 6304;  // floats per tile of learned-proposal gradient partials
 
 }  // namespace ym
 
@@ -82,7 +83,41 @@ struct ym_ensemble {
     size_t events_used[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 };
 
+// A learned-proposal model on one device (include/ym_learned.h).
+struct ym_proposal_model {
+    int32_t device = 0;
+    float *d_params = nullptr;             // YM_LP_PARAMS fp32 master parameters
+    float *d_adam_m = nullptr;
+    float *d_adam_v = nullptr;
+    int64_t adam_step = 0;
+    uint8_t *d_image = nullptr;            // BF16 weights in the shared-memory tile layout
+    unsigned *d_error = nullptr;           // bit 0: a tensor-core wait gave up
+    // Training and inspection buffers, grown on demand.
+    float *d_feat = nullptr;               // [rows][16]
+    float *d_mrec = nullptr;               // [rows][18]
+    float *d_b3 = nullptr;                 // [rows], negative marks a padding row
+    float *d_y = nullptr;                  // [rows][16]
+    int64_t row_capacity = 0;
+    float *d_partial = nullptr;            // [tiles][kLpPartialStride]
+    int64_t partial_capacity = 0;
+    float *d_grad = nullptr;               // YM_LP_PARAMS
+    double *d_objective = nullptr;         // per training step
+    int64_t objective_capacity = 0;
+    cudaStream_t stream = nullptr;
+};
+
 namespace ym {
+
+// learned.cu
+cudaError_t launch_lp_records(ym_ensemble *e, int parity, int mu, float *feat, float *m, float *b3);
+cudaError_t launch_lp_image(ym_proposal_model *m, cudaStream_t st);
+cudaError_t launch_lp_forward(ym_proposal_model *m, const float *feat, int64_t n, float *y,
+                              cudaStream_t st);
+cudaError_t launch_lp_grad(ym_proposal_model *m, const float *feat, const float *mrec,
+                           const float *b3, int64_t n, cudaStream_t st);
+cudaError_t launch_lp_adam(ym_proposal_model *m, int64_t n_tiles, int64_t n_valid, float lr,
+                           int update, float *grad_out, double *objective_out, cudaStream_t st);
+cudaError_t launch_lp_sweep(ym_ensemble *e, ym_proposal_model *m, int parity, int mu);
 
 // Launchers implemented in su3_f64.cu (return a cudaError_t).
 cudaError_t launch_su3_identity(ym_ensemble *e);

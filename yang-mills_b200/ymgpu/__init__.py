@@ -9,9 +9,10 @@ a compute entry point without the built ``libymgpu.so`` raises.
 from ._lib import LIB_PATH, lib
 from .ensemble import Ensemble, F32_TWO_ROW, F64, ORDERED, SU2, SU3, UNIFORM
 from .errors import YmError
-from . import glueball, su2_ensemble, su3_ensemble, su3_lattice
+from . import glueball, learned, su2_ensemble, su3_ensemble, su3_lattice
+from .learned import ProposalModel
 from .su3_lattice import Su3Lattice4
 
 __all__ = ["Ensemble", "Su3Lattice4", "YmError", "lib", "LIB_PATH", "su2_ensemble",
            "su3_ensemble", "su3_lattice", "glueball", "SU2", "SU3", "F64", "F32_TWO_ROW", "ORDERED",
-           "UNIFORM"]
+           "UNIFORM", "learned", "ProposalModel"]

@@ -67,10 +67,21 @@ SIGNATURES = {
     "ym_su2_max_unit_residual": [VP, P(f64)],
     "ym_profile_enable": [VP, i32],
     "ym_profile_read": [VP, i32, P(f64), P(i64)],
+    # learned proposal (include/ym_learned.h)
+    "ym_model_create": [i32, u64, f64, P(VP)],
+    "ym_model_destroy": [VP],
+    "ym_model_get_params": [VP, P(C.c_float)],
+    "ym_model_set_params": [VP, P(C.c_float)],
+    "ym_model_forward": [VP, P(C.c_float), i64, P(C.c_float)],
+    "ym_model_gradient": [VP, P(C.c_float), P(C.c_float), P(f64), i64, P(f64), P(C.c_float)],
+    "ym_learned_records": [VP, i32, i32, P(C.c_float), P(C.c_float), P(f64), P(i64)],
+    "ym_model_train": [VP, VP, i64, i64, f64, f64, P(f64)],
+    "ym_su3_learned_sweeps": [VP, VP, i64],
+    "ym_su3_learned_measured_sweeps": [VP, VP, i64, i64, P(f64)],
 }
 
 KERNEL_IDS = {"su3_metropolis": 0, "plaquette": 1, "su2_heatbath": 2, "su2_overrelax": 3,
-              "stout": 4, "operators": 5, "aux": 6}
+              "stout": 4, "operators": 5, "aux": 6, "learned": 7}
 
 
 class ChainDiagnostics(C.Structure):
