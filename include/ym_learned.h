@@ -11,8 +11,10 @@
  * with the link gives the local plaquette sum, ReTr(U A)), a small network
  * maps sixteen gauge-invariant features of A alone to eight generator
  * logits and one angle-scale output.  Each of the visit's eight hits draws
- * a generator a ~ softmax(logits) from bits 52..62 of its angle word, an
- * angle theta on the reference's paired grid with half width
+ * a generator a with probability p_a = F/8 + (1 - F) softmax(logits)_a
+ * (F = YM_LP_GENERATOR_FLOOR keeps every direction in play, so the chain
+ * stays ergodic however the logits train) from bits 52..62 of its angle
+ * word, an angle theta on the reference's paired grid with half width
  * s = SCALE_MIN + (SCALE_MAX - SCALE_MIN) * sigmoid(y8), proposes
  * exp(i theta T^a) U and accepts iff u < exp(-max(dS, 0)) with dS in
  * binary64.  A is fixed during the visit and the features do not depend on
@@ -68,6 +70,7 @@ enum {
 
 #define YM_LP_SCALE_MIN 0.05
 #define YM_LP_SCALE_MAX 2.5
+#define YM_LP_GENERATOR_FLOOR 0.5
 
 typedef struct ym_ensemble ym_ensemble;
 typedef struct ym_proposal_model ym_proposal_model;

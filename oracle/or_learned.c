@@ -105,18 +105,27 @@ int or_lp_forward(const float *params, const float *x, int64_t n, double *y) {
     return YM_OK;
 }
 
-/* Generator probabilities and angle half width from the outputs. */
-static void proposal_of(const double y[16], double p[8], double *s, double *sig) {
+/* Softmax of the logits (q), generator probabilities p = F/8 + (1-F) q and
+ * angle half width from the outputs. */
+static void proposal_q(const double y[16], double q[8], double p[8], double *s, double *sig) {
     double mx = y[0];
     for (int a = 1; a < 8; ++a) mx = fmax(mx, y[a]);
     double z = 0.0;
     for (int a = 0; a < 8; ++a) {
-        p[a] = exp(y[a] - mx);
-        z += p[a];
+        q[a] = exp(y[a] - mx);
+        z += q[a];
     }
-    for (int a = 0; a < 8; ++a) p[a] /= z;
+    for (int a = 0; a < 8; ++a) {
+        q[a] /= z;
+        p[a] = YM_LP_GENERATOR_FLOOR / 8.0 + (1.0 - YM_LP_GENERATOR_FLOOR) * q[a];
+    }
     *sig = 1.0 / (1.0 + exp(-y[8]));
     *s = YM_LP_SCALE_MIN + (YM_LP_SCALE_MAX - YM_LP_SCALE_MIN) * *sig;
+}
+
+static void proposal_of(const double y[16], double p[8], double *s, double *sig) {
+    double q[8];
+    proposal_q(y, q, p, s, sig);
 }
 
 int or_lp_proposal(const double *y16, double *p8, double *scale) {
@@ -154,8 +163,8 @@ static void retr_rotated(int g, const mat3 *mm, double theta, double *f, double 
 
 /* E of one record and dE/dy for outputs 0..8. */
 static double objective_row(const double y[16], const mat3 *m, double beta, double dy[9]) {
-    double p[8], s, sig;
-    proposal_of(y, p, &s, &sig);
+    double p[8], q[8], s, sig;
+    proposal_q(y, q, p, &s, &sig);
     const double b3 = beta / 3.0;
     const double tr = m->m[0][0].re + m->m[1][1].re + m->m[2][2].re;
     const int K = YM_LP_QUADRATURE;
@@ -179,7 +188,9 @@ static double objective_row(const double y[16], const mat3 *m, double beta, doub
         E += p[a] * J[a];
         dEs += p[a] * dJ[a];
     }
-    for (int a = 0; a < 8; ++a) dy[a] = p[a] * (J[a] - E);
+    double Eq = 0.0;
+    for (int a = 0; a < 8; ++a) Eq += q[a] * J[a];
+    for (int a = 0; a < 8; ++a) dy[a] = (1.0 - YM_LP_GENERATOR_FLOOR) * q[a] * (J[a] - Eq);
     dy[8] = dEs * (YM_LP_SCALE_MAX - YM_LP_SCALE_MIN) * sig * (1.0 - sig);
     return E;
 }

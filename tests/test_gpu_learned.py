@@ -4,14 +4,29 @@ then what training buys over plain Metropolis at equal plaquette.
 
 Tolerances: the device network accumulates in FP32 where the oracle sums in
 binary64 over the same BF16-rounded operands, so an activation can land on
-the other side of a BF16 rounding boundary; outputs agree to 2e-3 (relative
-to max(1, |y|)), gradients to 3% of their norm, the objective to 1e-4
-relative.  Features and M = U A come from binary32 staples: 2e-5 of their
+the other side of a BF16 rounding boundary; outputs agree to 1e-5 (relative
+to max(1, |y|)) in at least 97% of rows and to 1e-2 in all, gradients to 3%
+of their norm, the objective to 1e-4 relative.  Features and M = U A come from binary32 staples: 2e-5 of their
 scale."""
 import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
+
+
+def plaquette_np(extents, links):
+    """Average plaquette of a reference-layout lattice (no unitarity checks)."""
+    u = links.reshape(*extents, 4, 3, 3)
+    tot = 0.0
+    for mu in range(4):
+        for nu in range(mu + 1, 4):
+            a = u[..., mu, :, :]
+            b = np.roll(u[..., nu, :, :], -1, axis=mu)
+            c = np.roll(u[..., mu, :, :], -1, axis=nu)
+            d = u[..., nu, :, :]
+            p = a @ b @ np.conj(np.swapaxes(c, -1, -2)) @ np.conj(np.swapaxes(d, -1, -2))
+            tot += np.trace(p, axis1=-2, axis2=-1).real.mean() / 3.0
+    return tot / 6.0
 
 
 def thermal_f32(extents, n_chains, sweeps=60, beta=6.0, seed=7):
@@ -21,7 +36,7 @@ def thermal_f32(extents, n_chains, sweeps=60, beta=6.0, seed=7):
     ens = ymgpu.Ensemble([extents] * n_chains, beta, seeds, precision=ymgpu.F32_TWO_ROW,
                          lift_reference_caps=True)
     ens.hot_start()
-    ens.metropolis_sweeps(0.8, sweeps, "uniform")
+    ens.metropolis_sweeps(1.0 if sweeps > 100 else 0.8, sweeps, "uniform")
     return ens
 
 
@@ -40,7 +55,11 @@ def test_forward_matches_oracle(oracle):
     assert y.shape == (x.shape[0], 16)
     assert np.all(y[:, 9:] == 0)
     err = np.abs(y - ref) / np.maximum(1.0, np.abs(ref))
-    assert err.max() <= 2e-3, err.max()
+    # exact up to FP32 accumulation, except rows where one hidden activation
+    # rounds to the neighbouring BF16 value
+    row_err = err.max(1)
+    assert np.mean(row_err <= 1e-5) >= 0.97, np.mean(row_err <= 1e-5)
+    assert row_err.max() <= 1e-2, row_err.max()
 
 
 def test_records_match_oracle(oracle):
@@ -96,8 +115,8 @@ def test_learned_sweep_matches_oracle(oracle):
         npr, nac = oracle.lp_cb_sweep(ext, links, 6.0, model.params, int(ens.seeds[0]), sweep)
     assert int(p1[0] - p0[0]) == npr == 8 * 4 * 256
     assert abs(int(a1[0] - a0[0]) - nac) <= 0.01 * npr
-    plaq_or = oracle.su3_average_plaquette(ext, links)
-    assert abs(plaq_dev - plaq_or) <= 2e-3
+    assert abs(plaq_dev - plaquette_np(ext, dev)) <= 1e-6
+    assert abs(plaquette_np(ext, dev) - plaquette_np(ext, links)) <= 2e-4
     # most links agree to binary32 accuracy (a borderline decision may diverge)
     close = np.abs(dev - links).reshape(len(links), -1).max(1) <= 1e-4
     assert close.mean() >= 0.97
@@ -121,8 +140,11 @@ def test_trained_proposal_beats_plain():
     import ymgpu
     from ymgpu.su2_ensemble import diagnostics
     nch, meas = 32, 1500
-    with thermal_f32([8, 8, 8, 8], nch, sweeps=300) as ens, ymgpu.ProposalModel(seed=13) as model:
-        model.train(ens, 400, sweeps_per_step=1, plain_angle=0.3, lr=3e-3)
+    # equilibrium first: wide proposals relax the plaquette fastest
+    with thermal_f32([8, 8, 8, 8], nch, sweeps=1500) as ens, ymgpu.ProposalModel(seed=13) as model:
+        hist = model.train(ens, 2000, sweeps_per_step=1, plain_angle=0.3, lr=3e-3)
+        f, _, _ = ymgpu.learned.records(ens, 0, 0)
+        p_gen, s_half = ymgpu.learned.proposal(model.forward(f))
         plain = ens.like()
         ens.copy_to(plain)
         model.sweeps(ens, 200)
@@ -136,4 +158,5 @@ def test_trained_proposal_beats_plain():
     m_l, m_p = s_l.mean(0), s_p.mean(0)
     err = np.hypot(m_l.std(ddof=1), m_p.std(ddof=1)) / np.sqrt(nch)
     assert abs(m_l.mean() - m_p.mean()) <= 4 * err, (m_l.mean(), m_p.mean(), err)
-    assert t_l < t_p / 1.5, (t_l, t_p)
+    info = (t_l, t_p, s_half.mean(), p_gen.mean(0), hist[:3], hist[-3:])
+    assert t_l < t_p / 1.5, info

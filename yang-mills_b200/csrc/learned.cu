@@ -187,11 +187,12 @@ __device__ __forceinline__ void proposal_from(const float y[16], float cum[7], f
         e[a] = __expf(y[a] - mx);
         z += e[a];
     }
-    const float iz = 1.f / z;
+    const float iz = (1.f - (float)YM_LP_GENERATOR_FLOOR) / z;
+    const float base = (float)YM_LP_GENERATOR_FLOOR * 0.125f;
     float c = 0.f;
 #pragma unroll
     for (int a = 0; a < 7; ++a) {
-        c += e[a] * iz;
+        c += base + e[a] * iz;
         cum[a] = c;
     }
     const float sig = 1.f / (1.f + __expf(-y[8]));
@@ -231,14 +232,18 @@ __device__ __forceinline__ float objective_row(const float y[16], const float *m
     float mx = y[0];
 #pragma unroll
     for (int a = 1; a < 8; ++a) mx = fmaxf(mx, y[a]);
-    float p[8], z = 0.f;
+    float q[8], p[8], z = 0.f;
 #pragma unroll
     for (int a = 0; a < 8; ++a) {
-        p[a] = expf(y[a] - mx);
-        z += p[a];
+        q[a] = expf(y[a] - mx);
+        z += q[a];
     }
+    constexpr float F = (float)YM_LP_GENERATOR_FLOOR;
 #pragma unroll
-    for (int a = 0; a < 8; ++a) p[a] /= z;
+    for (int a = 0; a < 8; ++a) {
+        q[a] /= z;
+        p[a] = F * 0.125f + (1.f - F) * q[a];
+    }
     const float sig = 1.f / (1.f + expf(-y[8]));
     const float s = (float)YM_LP_SCALE_MIN + (float)(YM_LP_SCALE_MAX - YM_LP_SCALE_MIN) * sig;
     const float tr = m[0] + m[8] + m[16];
@@ -266,8 +271,11 @@ __device__ __forceinline__ float objective_row(const float y[16], const float *m
         E += p[a] * J[a];
         dEs += p[a] * (dj / (2.f * K));
     }
+    float Eq = 0.f;
 #pragma unroll
-    for (int a = 0; a < 8; ++a) dy[a] = p[a] * (J[a] - E);
+    for (int a = 0; a < 8; ++a) Eq += q[a] * J[a];
+#pragma unroll
+    for (int a = 0; a < 8; ++a) dy[a] = (1.f - F) * q[a] * (J[a] - Eq);
     dy[8] = dEs * (float)(YM_LP_SCALE_MAX - YM_LP_SCALE_MIN) * sig * (1.f - sig);
     return E;
 }

@@ -27,6 +27,7 @@ N_OUTPUTS = 16
 N_PARAMS = 6288
 OFFSETS = {"W1": 0, "b1": 1024, "W2": 1088, "b2": 5184, "W3": 5248, "b3": 6272}
 SCALE_MIN, SCALE_MAX = 0.05, 2.5
+GENERATOR_FLOOR = 0.5
 
 
 def _fp(a: np.ndarray):
@@ -130,6 +131,6 @@ def proposal(outputs):
     """Generator probabilities [n, 8] and angle half widths [n] from outputs."""
     y = np.asarray(outputs, np.float64).reshape(-1, N_OUTPUTS)
     z = np.exp(y[:, :8] - y[:, :8].max(1, keepdims=True))
-    p = z / z.sum(1, keepdims=True)
+    p = GENERATOR_FLOOR / 8 + (1 - GENERATOR_FLOOR) * z / z.sum(1, keepdims=True)
     s = SCALE_MIN + (SCALE_MAX - SCALE_MIN) / (1.0 + np.exp(-y[:, 8]))
     return p, s
