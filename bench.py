@@ -2,14 +2,21 @@
 """Throughput of the B200 lattice gauge engine on its headline workload.
 
 Workload (one GPU): SU(3) Wilson action, periodic 32^4, beta = 6.0, FP64
-links, Haar hot start, single-generator Metropolis with the reference's
-eight ordered generator hits per link visit and the paired angle grid of
-half width 0.3, updated over an even/odd checkerboard.  One step = one full
-sweep of every link followed by an average-plaquette measurement.  The
-lattice (604 MB) is larger than the 126 MB L2, so no flush is needed between
-steps.  ``value`` is link updates/s (one link visit = eight proposals) over
-all GPUs; the plaquette series of the timed steps gives the plaquette ESS/s
-through the reference's autocorrelation estimator.
+links, Haar hot start thermalised by wide-angle sweeps, single-generator
+Metropolis with the reference's eight ordered generator hits per link visit
+and the paired angle grid of half width 0.3, updated over an even/odd
+checkerboard.  One step = one full sweep of every link followed by an
+average-plaquette measurement.  The lattice (604 MB) is larger than the
+126 MB L2, so no flush is needed between steps.  ``value`` is link updates/s
+(one link visit = eight proposals) over all GPUs.
+
+Beside it: the same steps with two-row binary32 links (``fp32_two_row``),
+with the learned proposal (``learned``: its network trained on the GPU on
+2000 configurations of the plain sampler), and the plaquette ESS/s of plain
+FP64, plain FP32 and learned FP32 sampling at the learned-proposal geometry
+(16 chains of 16^4 in one handle, the total volume of 32^4), each judged by
+the reference's autocorrelation estimator (su2_ensemble.rs:375-463) on
+per-chain plaquette series.
 
 ``--impl reference`` times the reference's own algorithm (the lexicographic
 single-stream Metropolis sweep with twelve-plaquette action differences,
@@ -36,8 +43,12 @@ UNIT = "link updates/s"
 EXTENTS = [32, 32, 32, 32]
 BETA = 6.0
 ANGLE = 0.3
-THERMALIZATION = 400                  # 3/4 at angle 1.0 (fast relaxation), 1/4 at ANGLE
-THERMALIZATION_ANGLE = 1.0
+THERMALIZATION = 1500                 # wide-angle sweeps from the hot start
+THERMALIZATION_ANGLE = 1.0            # the plaquette relaxes fastest at wide angles
+ESS_CHAINS, ESS_EXTENTS = 16, [16, 16, 16, 16]
+ESS_SWEEPS = 2000                     # measured sweeps per sampler (one plaquette each)
+TRAIN_STEPS = 2000                    # configurations the plain sampler generates for training
+TRAIN_LR = 3e-3
 MASTER_SEED = 0x2C02198105010002
 LINK_BYTES = 144                      # FP64 3x3 complex
 LINKS_PER_UPDATE = 9                  # 8 link reads + 1 write per checkerboard update
@@ -52,6 +63,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--thermalization", type=int, default=THERMALIZATION)
+    ap.add_argument("--ess-sweeps", type=int, default=ESS_SWEEPS)
+    ap.add_argument("--train-steps", type=int, default=TRAIN_STEPS)
     return ap.parse_args()
 
 
@@ -221,6 +234,7 @@ def main():
     import torch.distributed as dist
     import ymgpu
     from ymgpu.su2_ensemble import diagnostics
+    from ymgpu.su3_ensemble import derive_su3_chain_seed
 
     torch.cuda.set_device(local)
     if world > 1:
@@ -232,7 +246,7 @@ def main():
         if world > 1:
             dist.barrier()
 
-    seed = ymgpu.su3_ensemble.derive_su3_chain_seed(MASTER_SEED, rank)
+    seed = derive_su3_chain_seed(MASTER_SEED, rank)
     volume = int(np.prod(EXTENTS))
     links = 4 * volume
     peak, peak_kind = measured_peaks()
@@ -244,17 +258,12 @@ def main():
             return float(t.item())
         return x
 
-    def run_leg(precision, link_bytes, sampler_clocks=False):
-        """Thermalise, then time args.steps steps (sweep [+ reunitarise] +
-        plaquette) with CUDA events on the handle's stream."""
-        ens = ymgpu.Ensemble([EXTENTS], BETA, seed, precision=precision,
-                             lift_reference_caps=True, device=local)
-        ens.hot_start()
-        wide = (3 * args.thermalization) // 4
-        ens.metropolis_sweeps(THERMALIZATION_ANGLE, wide)
-        ens.metropolis_sweeps(ANGLE, args.thermalization - wide)
+    def timed_leg(ens, step, link_bytes, kernel, sampler_clocks=False):
+        """W warm-up steps, then args.steps steps (step() = one sweep) each
+        followed by the plaquette, timed with CUDA events on the handle's
+        stream; per-launch time of the dominant kernel from event pairs."""
         for _ in range(args.warmup):
-            ens.metropolis_sweeps(ANGLE, 1)
+            step()
             ens.average_plaquette()
         ens.synchronize()
         stream = torch.cuda.ExternalStream(ens.stream(), device=local)
@@ -270,7 +279,7 @@ def main():
             sampler.wait_first()
         start.record(stream)
         for _ in range(args.steps):
-            ens.metropolis_sweeps(ANGLE, 1)     # two-row handles reunitarise inside the sweep
+            step()
             plaq.append(float(ens.average_plaquette()[0]))
         stop.record(stream)
         stop.synchronize()
@@ -280,39 +289,93 @@ def main():
             sampler.__exit__(None, None, None)
         barrier()
         ms = max_over_ranks(start.elapsed_time(stop))
-        sweep_ms, sweep_launches = ens.profile_read("su3_metropolis")
+        k_ms, k_launches = ens.profile_read(kernel)
         ens.profile(False)
         p1, a1 = ens.accounting()
-        # plaquette ESS/s through the reference estimator (su2_ensemble.rs:375-463)
-        max_lag = max(1, min(len(plaq) // 4, 50))
-        diag, _ = diagnostics(np.array(plaq), max_lag)
-        # roofline of the dominant kernel (one checkerboard sub-sweep launch)
-        launch_s = sweep_ms * 1e-3 / max(1, sweep_launches)
-        achieved = (volume // 2) * LINKS_PER_UPDATE * link_bytes / launch_s / 1e9
-        return ens, {
-            "ms": ms, "value": world * links * args.steps / (ms * 1e-3),
-            "plaq": plaq, "diag": diag,
-            "ess_per_s": world * diag.effective_sample_size / (ms * 1e-3),
+        launch_s = k_ms * 1e-3 / max(1, k_launches)
+        bytes_per_launch = (volume // 2) * LINKS_PER_UPDATE * link_bytes
+        achieved = bytes_per_launch / launch_s / 1e9
+        return {
+            "ms": ms, "value": world * links * args.steps / (ms * 1e-3), "plaq": plaq,
             "acceptance": float((a1 - a0)[0]) / float((p1 - p0)[0]),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
-                         "launch_ms": launch_s * 1e3, "kernel_share_of_step": sweep_ms / ms,
-                         "bytes_per_launch": (volume // 2) * LINKS_PER_UPDATE * link_bytes},
+                         "launch_ms": launch_s * 1e3, "kernel_share_of_step": k_ms / ms,
+                         "bytes_per_launch": bytes_per_launch},
             "clocks": sampler.summary() if sampler else None,
         }
 
-    # binary32 two-row leg (BASELINE configs[2] link algebra), reported beside
-    f32_ens, f32 = run_leg(ymgpu.F32_TWO_ROW, 48)
-    f32_ens.close()
-    ens, leg = run_leg(ymgpu.F64, LINK_BYTES, sampler_clocks=True)
-    ms, plaq, diag = leg["ms"], leg["plaq"], leg["diag"]
-    step_ms = ms / args.steps
-    value = leg["value"]
-    ess_per_s = leg["ess_per_s"]
-    clocks = leg["clocks"]
+    # one thermalised 32^4 lattice (two-row binary32; wide-angle sweeps relax
+    # the plaquette fastest), shared by all legs
+    t32 = ymgpu.Ensemble([EXTENTS], BETA, seed, precision=ymgpu.F32_TWO_ROW,
+                         lift_reference_caps=True, device=local)
+    t32.hot_start()
+    t32.metropolis_sweeps(THERMALIZATION_ANGLE, args.thermalization, "uniform")
+
+    # learned proposal: network trained on configurations of the plain
+    # sampler at the learned-proposal geometry (16 x 16^4)
+    ess_seeds = [derive_su3_chain_seed(MASTER_SEED ^ 0x16, rank * ESS_CHAINS + i)
+                 for i in range(ESS_CHAINS)]
+    e16 = ymgpu.Ensemble([ESS_EXTENTS] * ESS_CHAINS, BETA, ess_seeds, precision=ymgpu.F32_TWO_ROW,
+                         lift_reference_caps=True, device=local)
+    e16.hot_start()
+    e16.metropolis_sweeps(THERMALIZATION_ANGLE, args.thermalization, "uniform")
+    model = ymgpu.ProposalModel(device=local, initial_scale=ANGLE)
+    e16.synchronize()
+    t0 = time.perf_counter()
+    train_hist = model.train(e16, args.train_steps, sweeps_per_step=1, plain_angle=ANGLE, lr=TRAIN_LR)
+    train_s = time.perf_counter() - t0
+    f_rec, _, _ = ymgpu.learned.records(e16, 0, 0)
+    p_gen, s_half = ymgpu.learned.proposal(model.forward(f_rec))
+
+    # FP32 plain leg (ordered generators, half width 0.3)
+    f32 = timed_leg(t32, lambda: t32.metropolis_sweeps(ANGLE, 1), 48, "su3_metropolis")
+    # learned leg from the same starting lattice
+    tl = t32.like()
+    t32.copy_to(tl)
+    lrn = timed_leg(tl, lambda: model.sweeps(tl, 1), 48, "learned")
+    tl.close()
+    # FP64 headline leg
+    ens = t32.like(precision=ymgpu.F64)
+    t32.convert_to(ens)
+    t32.close()
+    leg = timed_leg(ens, lambda: ens.metropolis_sweeps(ANGLE, 1), LINK_BYTES, "su3_metropolis",
+                    sampler_clocks=True)
+    ms, plaq = leg["ms"], leg["plaq"]
     roofline = dict(leg["roofline"])
     roofline.update({"traffic": ncu_traffic_per_launch(),
                      "kernel": "k_su3_metropolis (one checkerboard sub-sweep)"})
+
+    # plaquette ESS/s of the three samplers at 16 x 16^4 from one equilibrated state
+    def ess_leg(e, run):
+        e.synchronize()
+        t = time.perf_counter()
+        series = run()
+        secs = time.perf_counter() - t
+        lag = max(1, min(500, series.shape[0] // 4))
+        diags = [diagnostics(series[:, c], lag)[0] for c in range(series.shape[1])]
+        ess = float(sum(d.effective_sample_size for d in diags))
+        means = series.mean(0)
+        return {"plaquette_ess_per_s": world * ess / secs, "seconds": secs,
+                "tau_int": float(np.mean([d.integrated_autocorrelation_time for d in diags])),
+                "plaquette_mean": float(means.mean()),
+                "plaquette_error": float(means.std(ddof=1) / np.sqrt(len(means))),
+                "link_updates_per_s": world * 4 * int(np.prod(ESS_EXTENTS)) * ESS_CHAINS *
+                                      series.shape[0] / secs}
+
+    e64 = e16.like(precision=ymgpu.F64)
+    e16.convert_to(e64)
+    e32p = e16.like()
+    e16.copy_to(e32p)
+    n = args.ess_sweeps
+    ess_f64 = ess_leg(e64, lambda: e64.measured_sweeps(ANGLE, n, 1, "ordered"))
+    ess_f32 = ess_leg(e32p, lambda: e32p.measured_sweeps(ANGLE, n, 1, "uniform"))
+    ess_lrn = ess_leg(e16, lambda: model.measured_sweeps(e16, n))
+    for e in (e64, e32p, e16):
+        e.close()
+    model.close()
+    sig = lambda a, b: abs(a["plaquette_mean"] - b["plaquette_mean"]) / np.hypot(
+        a["plaquette_error"], b["plaquette_error"])
 
     # end to end through the C ABI with host buffers: upload the lattice from
     # pinned host memory, sweep, measure, download the lattice
@@ -339,32 +402,53 @@ def main():
     if rank == 0:
         cpu = None if (args.no_cpu_baseline or world > 1) else cpu_baseline()
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
+            "metric": METRIC, "value": leg["value"], "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": "SU(3) 32^4 beta=6.0 plain FP64 Metropolis (configs[2] "
-                                   "geometry), 8 ordered hits/link, angle 0.3, Haar hot start "
-                                   f"+ {args.thermalization} untimed thermalization sweeps "
-                                   "(3/4 at angle 1.0, 1/4 at 0.3)",
+            "config": {"workload": "SU(3) 32^4 beta=6.0 plain FP64 Metropolis, 8 ordered hits/link, "
+                                   f"half width 0.3, Haar hot start + {args.thermalization} untimed "
+                                   "wide-angle sweeps",
                        "lattice": "32^4", "global_batch": world, "parallelism": f"replicas x{world}",
                        "l2": "inputs 604 MB > 126 MB L2 (no flush)",
                        "step": "1 checkerboard sweep + average plaquette"},
             "plaquette_mean": float(np.mean(plaq)),
-            "plaquette_ess_per_s": ess_per_s,
-            "plaquette_tau_int": diag.integrated_autocorrelation_time,
             "acceptance": leg["acceptance"],
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": int(args.steps * 11),
-            "clocks": clocks,
+            "clocks": leg["clocks"],
             "fp32_two_row": {
                 "value": f32["value"], "unit": UNIT, "dtype": "f32 links, f64 dS/accept/plaquette",
                 "ms_per_step": f32["ms"] / args.steps,
                 "step": "1 checkerboard sweep + FP64 reunitarisation + average plaquette",
-                "plaquette_mean": float(np.mean(f32["plaq"])),
-                "plaquette_minus_f64": float(np.mean(f32["plaq"]) - np.mean(plaq)),
-                "plaquette_ess_per_s": f32["ess_per_s"], "acceptance": f32["acceptance"],
+                "plaquette_mean": float(np.mean(f32["plaq"])), "acceptance": f32["acceptance"],
                 "roofline": f32["roofline"]},
+            "learned": {
+                "value": lrn["value"], "unit": UNIT, "ms_per_step": lrn["ms"] / args.steps,
+                "dtype": "f32 links, bf16 network (fp32 accumulate), f64 dS/accept/plaquette",
+                "step": "1 learned checkerboard sweep + FP64 reunitarisation + average plaquette",
+                "plaquette_mean": float(np.mean(lrn["plaq"])), "acceptance": lrn["acceptance"],
+                "roofline": dict(lrn["roofline"], kernel="k_lp_sweep (staple, features, tcgen05 "
+                                                         "network, 8 hits; one sub-sweep)"),
+                "training": {"configurations": args.train_steps, "seconds": train_s,
+                             "geometry": f"{ESS_CHAINS} x 16^4", "lr": TRAIN_LR,
+                             "objective_first": float(np.mean(train_hist[:20])),
+                             "objective_last": float(np.mean(train_hist[-20:])),
+                             "mean_half_width": float(np.mean(s_half)),
+                             "mean_generator_probabilities": [float(v) for v in p_gen.mean(0)]}},
+            "ess": {
+                "geometry": f"{ESS_CHAINS} chains x 16^4 (total volume of 32^4), beta=6.0, "
+                            f"{n} measured sweeps per sampler from one equilibrated state",
+                "estimator": "reference diagnostics (initial positive window), per chain, summed",
+                "plain_f64_ordered_0.3": ess_f64, "plain_f32_uniform_0.3": ess_f32,
+                "learned_f32": ess_lrn,
+                "learned_vs_plain_f64": ess_lrn["plaquette_ess_per_s"] / ess_f64["plaquette_ess_per_s"],
+                "learned_vs_plain_f32": ess_lrn["plaquette_ess_per_s"] / ess_f32["plaquette_ess_per_s"],
+                "learned_vs_plain_f64_with_training": (
+                    (ess_lrn["plaquette_ess_per_s"] * ess_lrn["seconds"]) /
+                    (ess_lrn["seconds"] + train_s)) / ess_f64["plaquette_ess_per_s"],
+                "plaquette_sigma_learned_vs_f64": float(sig(ess_lrn, ess_f64)),
+                "plaquette_sigma_f32_vs_f64": float(sig(ess_f32, ess_f64))},
         }
         print(json.dumps(line))
     if world > 1:
