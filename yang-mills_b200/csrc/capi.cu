@@ -917,7 +917,7 @@ namespace {
 
 void free_model(ym_proposal_model *m) {
     void *ptrs[] = {m->d_params, m->d_adam_m, m->d_adam_v, m->d_image, m->d_error, m->d_feat,
-                    m->d_mrec, m->d_b3, m->d_y, m->d_partial, m->d_grad, m->d_objective};
+                    m->d_mrec, m->d_b3, m->d_y, m->d_partial, m->d_groups, m->d_grad, m->d_objective};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (m->stream) cudaStreamDestroy(m->stream);
@@ -946,9 +946,13 @@ cudaError_t ensure_rows(ym_proposal_model *m, int64_t rows) {
 cudaError_t ensure_partials(ym_proposal_model *m, int64_t tiles) {
     if (tiles <= m->partial_capacity) return cudaSuccess;
     if (m->d_partial) cudaFree(m->d_partial);
+    if (m->d_groups) cudaFree(m->d_groups);
     m->d_partial = nullptr;
+    m->d_groups = nullptr;
     m->partial_capacity = 0;
     cudaError_t err = dalloc(&m->d_partial, (size_t)(tiles * ym::kLpPartialStride));
+    if (err == cudaSuccess)
+        err = dalloc(&m->d_groups, (size_t)(ym::lp_reduce_groups(tiles) * ym::kLpPartialStride));
     if (err == cudaSuccess) m->partial_capacity = tiles;
     return err;
 }

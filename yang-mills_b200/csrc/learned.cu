@@ -531,24 +531,38 @@ __global__ void k_lp_image(const float *__restrict__ params, uint8_t *__restrict
         *reinterpret_cast<__nv_bfloat16 *>(image + off) = __float2bfloat16_rn(params[p]);
 }
 
-// Gradient reduction over tiles in tile order, then Adam (bias-corrected)
-// and the BF16 image.  grad_out (optional) receives the mean gradient;
-// objective_out (optional) the mean objective.
-__global__ void k_lp_adam(const float *__restrict__ partial, int64_t n_tiles, int64_t stride,
+// Gradient reduction in two fixed-order stages (groups of kGroup tiles, then
+// the groups in order), so the result does not depend on scheduling.
+constexpr int kGroup = 64;
+
+__global__ void k_lp_reduce_groups(const float *__restrict__ partial, int64_t n_tiles, int64_t stride,
+                                   double *__restrict__ groups) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p > YM_LP_PARAMS) return;                 // p == YM_LP_PARAMS is the objective
+    const int64_t g = blockIdx.y, t0 = g * kGroup;
+    const int64_t t1 = t0 + kGroup < n_tiles ? t0 + kGroup : n_tiles;
+    double acc = 0.0;
+    for (int64_t t = t0; t < t1; ++t) acc += (double)partial[t * stride + p];
+    groups[g * stride + p] = acc;
+}
+
+// Sum of the groups, then Adam (bias-corrected) and the BF16 image.
+// grad_out (optional) receives the mean gradient; objective_out (optional)
+// the mean objective.
+__global__ void k_lp_adam(const double *__restrict__ groups, int64_t n_groups, int64_t stride,
                           double inv_n, float *__restrict__ params, float *__restrict__ am,
                           float *__restrict__ av, int64_t step, float lr, int update,
                           uint8_t *__restrict__ image, float *__restrict__ grad_out,
                           double *__restrict__ objective_out) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p == 0 && objective_out) {
-        double e = 0.0;
-        for (int64_t t = 0; t < n_tiles; ++t) e += (double)partial[t * stride + YM_LP_PARAMS];
-        *objective_out = e * inv_n;
-    }
-    if (p >= YM_LP_PARAMS) return;
+    if (p > YM_LP_PARAMS) return;
     double g = 0.0;
-    for (int64_t t = 0; t < n_tiles; ++t) g += (double)partial[t * stride + p];
-    float gf = is_padding_param(p) ? 0.f : (float)(g * inv_n);
+    for (int64_t t = 0; t < n_groups; ++t) g += groups[t * stride + p];
+    if (p == YM_LP_PARAMS) {
+        if (objective_out) *objective_out = g * inv_n;
+        return;
+    }
+    const float gf = is_padding_param(p) ? 0.f : (float)(g * inv_n);
     if (grad_out) grad_out[p] = gf;
     if (!update) return;
     const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
@@ -558,7 +572,7 @@ __global__ void k_lp_adam(const float *__restrict__ partial, int64_t n_tiles, in
     av[p] = v;
     const float mh = m / (1.f - powf(b1, (float)step));
     const float vh = v / (1.f - powf(b2, (float)step));
-    float w = is_padding_param(p) ? 0.f : params[p] - lr * mh / (sqrtf(vh) + eps);
+    const float w = is_padding_param(p) ? 0.f : params[p] - lr * mh / (sqrtf(vh) + eps);
     params[p] = w;
     const int off = image_offset(p);
     if (off >= 0) *reinterpret_cast<__nv_bfloat16 *>(image + off) = __float2bfloat16_rn(w);
@@ -678,9 +692,13 @@ cudaError_t launch_lp_grad(ym_proposal_model *m, const float *feat, const float 
 cudaError_t launch_lp_adam(ym_proposal_model *m, int64_t n_tiles, int64_t n_valid, float lr,
                            int update, float *grad_out, double *objective_out, cudaStream_t st) {
     if (update) m->adam_step += 1;
-    lp::k_lp_adam<<<(YM_LP_PARAMS + 255) / 256, 256, 0, st>>>(
-        m->d_partial, n_tiles, kLpPartialStride, 1.0 / (double)n_valid, m->d_params, m->d_adam_m,
-        m->d_adam_v, m->adam_step, lr, update, m->d_image, grad_out, objective_out);
+    const int64_t n_groups = lp_reduce_groups(n_tiles);
+    const unsigned blocks = (YM_LP_PARAMS + 1 + 255) / 256;
+    lp::k_lp_reduce_groups<<<dim3(blocks, (unsigned)n_groups), 256, 0, st>>>(m->d_partial, n_tiles,
+                                                                           kLpPartialStride, m->d_groups);
+    lp::k_lp_adam<<<blocks, 256, 0, st>>>(m->d_groups, n_groups, kLpPartialStride, 1.0 / (double)n_valid,
+                                          m->d_params, m->d_adam_m, m->d_adam_v, m->adam_step, lr,
+                                          update, m->d_image, grad_out, objective_out);
     return cudaGetLastError();
 }
 

@@ -15,6 +15,8 @@ namespace ym {
 constexpr int kSweepThreads = 128;   // threads per tile of a sub-sweep
 constexpr int kSiteThreads = 128;    // threads per tile of a measurement
 constexpr int64_t kLpPartialStride = 6304;  // floats per tile of learned-proposal gradient partials
+// Groups of 64 tiles in the first stage of the gradient reduction.
+inline int64_t lp_reduce_groups(int64_t tiles) { return (tiles + 63) / 64; }
 
 }  // namespace ym
 
@@ -100,6 +102,7 @@ struct ym_proposal_model {
     int64_t row_capacity = 0;
     float *d_partial = nullptr;            // [tiles][kLpPartialStride]
     int64_t partial_capacity = 0;
+    double *d_groups = nullptr;            // [ceil(tiles / 64)][kLpPartialStride]
     float *d_grad = nullptr;               // YM_LP_PARAMS
     double *d_objective = nullptr;         // per training step
     int64_t objective_capacity = 0;
