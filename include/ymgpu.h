@@ -109,6 +109,20 @@ int32_t ym_su3_metropolis_sweeps(ym_ensemble *ens, double proposal_angle, int32_
 int32_t ym_su3_measured_sweeps(ym_ensemble *ens, double proposal_angle, int32_t generator_mode,
                                int64_t n_measurements, int64_t sweeps_per_measurement,
                                double *series);
+/* Sweep path of SU(3) FP64 handles (no reference counterpart).  When every
+ * chain is small enough for its links to sit in one CTA's shared memory
+ * (4^4 and similar), sweeps can run chain-resident: one launch does many
+ * whole sweeps of every chain in shared memory.  YM_PATH_AUTO (the default)
+ * times a few sweeps on each path in the first call long enough to tell
+ * them apart and keeps the faster; YM_PATH_TILED and YM_PATH_RESIDENT force
+ * one (RESIDENT fails with YM_ERR_INVALID_ARGUMENT when a chain does not
+ * fit or the handle is not SU(3) FP64).  Both paths give the same bits:
+ * links, accept counts and measured plaquettes. */
+enum { YM_PATH_AUTO = -1, YM_PATH_TILED = 0, YM_PATH_RESIDENT = 1 };
+int32_t ym_ensemble_set_sweep_path(ym_ensemble *ens, int32_t path);
+/* The path in use: YM_PATH_AUTO while not yet decided. */
+int32_t ym_ensemble_get_sweep_path(ym_ensemble *ens, int32_t *path);
+
 /* Accumulated proposals/accepts per chain since creation or reset
  * (MetropolisAccounting su3_ensemble.rs:117-121). */
 int32_t ym_su3_accounting(ym_ensemble *ens, uint64_t *proposals, uint64_t *accepts);

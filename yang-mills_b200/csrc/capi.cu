@@ -198,6 +198,32 @@ cudaError_t timed(ym_ensemble *e, int kernel, F launch) {
     return err;
 }
 
+// Device time of run() on the handle's stream, in milliseconds.
+template <class F>
+cudaError_t time_on_stream(ym_ensemble *e, F run, float *ms) {
+    cudaEvent_t a = nullptr, b = nullptr;
+    cudaError_t err = cudaEventCreate(&a);
+    if (err == cudaSuccess) err = cudaEventCreate(&b);
+    if (err == cudaSuccess) err = cudaEventRecord(a, e->stream);
+    if (err == cudaSuccess) err = run();
+    if (err == cudaSuccess) err = cudaEventRecord(b, e->stream);
+    if (err == cudaSuccess) err = cudaEventSynchronize(b);
+    if (err == cudaSuccess) err = cudaEventElapsedTime(ms, a, b);
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+    return err;
+}
+
+// The chain-resident path applies to SU(3) FP64 handles whose every chain
+// fits one CTA's shared memory; profiled runs keep the tiled launches so
+// each sub-sweep keeps its event pair.
+bool resident_candidate(const ym_ensemble *e) {
+    return e->group == YM_GROUP_SU3 && e->precision == YM_PREC_F64 && !e->profiling &&
+           e->resident_choice != 0 && ym::resident_fits(e);
+}
+
+constexpr int64_t kTuneSweeps = 4;   // sweeps timed per path when choosing
+
 }  // namespace
 
 extern "C" {
@@ -453,10 +479,31 @@ int32_t ym_su3_metropolis_sweeps(ym_ensemble *e, double angle, int32_t generator
         return ym::launch_advance_sweep(e);
     };
     int64_t done = 0;
+    // Small chains: the first call long enough times kTuneSweeps sweeps on
+    // each path and keeps the faster; the rest go to the chosen path.
+    if (resident_candidate(e)) {
+        if (e->resident_choice < 0 && n_sweeps >= 2 * kTuneSweeps) {
+            float t_tiled = 0.f, t_res = 0.f;
+            YM_CUDA(time_on_stream(e, [&] {
+                cudaError_t err = cudaSuccess;
+                for (int64_t k = 0; k < kTuneSweeps && err == cudaSuccess; ++k) err = one_sweep();
+                return err;
+            }, &t_tiled));
+            YM_CUDA(time_on_stream(e, [&] {
+                return ym::launch_su3_resident(e, angle, generator_mode, 1, kTuneSweeps, nullptr);
+            }, &t_res));
+            e->resident_choice = t_res < t_tiled ? 1 : 0;
+            done = 2 * kTuneSweeps;
+        }
+        if (e->resident_choice == 1 && done < n_sweeps) {
+            YM_CUDA(ym::launch_su3_resident(e, angle, generator_mode, 1, n_sweeps - done, nullptr));
+            done = n_sweeps;
+        }
+    }
     // Batches of kGraphSweeps sweeps replay one captured graph (9 launches
     // per sweep become one graph launch per batch).  Timed runs launch
     // directly so each kernel keeps its event pair.
-    if (!e->profiling && n_sweeps >= kGraphSweeps) {
+    if (!e->profiling && n_sweeps - done >= kGraphSweeps) {
         if (!e->sweep_graph || e->sweep_graph_angle != angle || e->sweep_graph_mode != generator_mode) {
             if (e->sweep_graph) cudaGraphExecDestroy(e->sweep_graph);
             e->sweep_graph = nullptr;
@@ -539,13 +586,57 @@ int32_t ym_su3_measured_sweeps(ym_ensemble *e, double angle, int32_t generator_m
         e->measure_graph_mode = generator_mode;
         e->measure_graph_stride = sweeps_per_measurement;
     }
-    for (int64_t m = 0; m < n_measurements; ++m) YM_CUDA(cudaGraphLaunch(e->measure_graph, e->stream));
+    int64_t m = 0;
+    if (resident_candidate(e)) {
+        // Rows written by the resident kernel go to row m of the series; the
+        // tiled graph continues from the device row counter.
+        if (e->resident_choice < 0 && n_measurements >= 2 && n_measurements * sweeps_per_measurement >= 2 * kTuneSweeps) {
+            float t_tiled = 0.f, t_res = 0.f;
+            YM_CUDA(time_on_stream(e, [&] { return cudaGraphLaunch(e->measure_graph, e->stream); }, &t_tiled));
+            YM_CUDA(time_on_stream(e, [&] {
+                return ym::launch_su3_resident(e, angle, generator_mode, 1, sweeps_per_measurement,
+                                               e->d_series + 1 * e->n_chains);
+            }, &t_res));
+            e->resident_choice = t_res < t_tiled ? 1 : 0;
+            m = 2;
+        }
+        if (e->resident_choice == 1 && m < n_measurements) {
+            YM_CUDA(ym::launch_su3_resident(e, angle, generator_mode, n_measurements - m, sweeps_per_measurement,
+                                            e->d_series + m * e->n_chains));
+            m = n_measurements;
+        }
+        if (m > 0 && m < n_measurements) {
+            const uint64_t row = (uint64_t)m;
+            YM_CUDA(cudaMemcpyAsync(e->d_series_row, &row, sizeof row, cudaMemcpyHostToDevice, e->stream));
+            YM_CUDA(cudaStreamSynchronize(e->stream));
+        }
+    }
+    for (; m < n_measurements; ++m) YM_CUDA(cudaGraphLaunch(e->measure_graph, e->stream));
     YM_CUDA(cudaMemcpyAsync(series, e->d_series, (size_t)(n_measurements * e->n_chains) * sizeof(double),
                             cudaMemcpyDeviceToHost, e->stream));
     YM_CUDA(cudaStreamSynchronize(e->stream));
     for (int64_t ch = 0; ch < e->n_chains; ++ch)
         e->proposals[ch] += (uint64_t)(n_measurements * sweeps_per_measurement) * 32u *
                             (uint64_t)e->chains[ch].volume;
+    return YM_OK;
+}
+
+int32_t ym_ensemble_set_sweep_path(ym_ensemble *e, int32_t path) {
+    if (!e) return YM_ERR_NULL_ARGUMENT;
+    if (path != YM_PATH_AUTO && path != YM_PATH_TILED && path != YM_PATH_RESIDENT) return YM_ERR_INVALID_ARGUMENT;
+    if (path == YM_PATH_RESIDENT) {
+        int32_t st = set_device(e);
+        if (st) return st;
+        if (e->group != YM_GROUP_SU3 || e->precision != YM_PREC_F64 || !ym::resident_fits(e))
+            return YM_ERR_INVALID_ARGUMENT;
+    }
+    e->resident_choice = path;
+    return YM_OK;
+}
+
+int32_t ym_ensemble_get_sweep_path(ym_ensemble *e, int32_t *path) {
+    if (!e || !path) return YM_ERR_NULL_ARGUMENT;
+    *path = e->resident_choice;
     return YM_OK;
 }
 

@@ -12,34 +12,12 @@
 
 #include "su3_exp.cuh"
 #include "su3_haar.cuh"
+#include "su3_sites.cuh"
 #include "ym_internal.hpp"
 
 namespace ym {
 
 // ------------------------------------------------------------ reductions
-
-template <bool kMax>
-__device__ __forceinline__ double block_reduce(double v) {
-    __shared__ double warp_vals[32];
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-        const double o = __shfl_down_sync(0xffffffffu, v, off);
-        v = kMax ? fmax(v, o) : v + o;
-    }
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (lane == 0) warp_vals[warp] = v;
-    __syncthreads();
-    const int nw = (blockDim.x + 31) >> 5;
-    if (warp == 0) {
-        v = lane < nw ? warp_vals[lane] : (kMax ? 0.0 : 0.0);
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) {
-            const double o = __shfl_down_sync(0xffffffffu, v, off);
-            v = kMax ? fmax(v, o) : v + o;
-        }
-    }
-    return v;   // valid in thread 0
-}
 
 // Sum of the six plaquette values (1/3) Re Tr P of each site, site order
 // (mu, nu) = (0,1),(0,2),(0,3),(1,2),(1,3),(2,3), per tile.
@@ -50,24 +28,7 @@ k_su3_plaquette(const ChainInfo *__restrict__ chains, const Tile *__restrict__ t
     const ChainInfo c = chains[tile.chain];
     const int64_t s = tile.start + threadIdx.x;
     double v = 0.0;
-    if (s < c.volume) {
-        const Coord x = decode_storage(c, s);
-        bool first = true;
-#pragma unroll 1
-        for (int mu = 0; mu < 3; ++mu) {
-            const m3 umu = load_su3(links, c, s, mu);
-            const Nb pm = step(c, x.x, x.lex, x.par, mu, +1);
-#pragma unroll 1
-            for (int nu = mu + 1; nu < 4; ++nu) {
-                const Nb pn = step(c, x.x, x.lex, x.par, nu, +1);
-                m3 p = mul(umu, load_su3(links, c, storage_index(c, pm.lex, pm.par), nu));
-                p = mul_adj(p, load_su3(links, c, storage_index(c, pn.lex, pn.par), mu));
-                const double val = retrace_mul_adj(p, load_su3(links, c, s, nu)) / 3.0;
-                v = first ? val : v + val;
-                first = false;
-            }
-        }
-    }
+    if (s < c.volume) v = site_plaquette_sum<false>(links, c, s);
     v = block_reduce<false>(v);
     if (threadIdx.x == 0) partial[blockIdx.x] = v;
 }

@@ -74,6 +74,9 @@ struct ym_ensemble {
     double measure_graph_angle = 0.0;
     int32_t measure_graph_mode = -1;
     int64_t measure_graph_stride = -1;
+    // Small-chain path choice: -1 not yet measured, 0 tiled launches, 1 the
+    // chain-resident kernel (picked by timing both on the first sweeps).
+    int32_t resident_choice = -1;
     double *d_series = nullptr;            // [measurement][chain]
     int64_t series_capacity = 0;           // rows
     uint64_t *d_series_row = nullptr;
@@ -128,6 +131,12 @@ cudaError_t launch_su3_from_aos(ym_ensemble *e, int64_t chain);
 cudaError_t launch_su3_to_aos(ym_ensemble *e, int64_t chain);
 cudaError_t launch_su3_metropolis(ym_ensemble *e, int parity, int mu, double angle, int uniform);
 cudaError_t launch_advance_sweep(ym_ensemble *e);
+// Chain-resident sweeps (su3_metropolis.cu): every chain small enough that
+// its links fit in one CTA's shared memory.  series (device, may be null)
+// receives the plaquette of every chain after each group of sweeps.
+bool resident_fits(const ym_ensemble *e);
+cudaError_t launch_su3_resident(ym_ensemble *e, double angle, int uniform, int64_t n_meas,
+                                int64_t sweeps_per_meas, double *series);
 cudaError_t launch_su3_plaquette(ym_ensemble *e);
 cudaError_t launch_su3_residuals(ym_ensemble *e);
 cudaError_t launch_su3_reference_sweeps(ym_ensemble *e, double angle, int64_t n_sweeps);

@@ -39,6 +39,8 @@ SIGNATURES = {
     "ym_ensemble_stream": [VP, P(VP)],
     "ym_su3_metropolis_sweeps": [VP, f64, i32, i64],
     "ym_su3_accounting": [VP, P(u64), P(u64)],
+    "ym_ensemble_set_sweep_path": [VP, i32],
+    "ym_ensemble_get_sweep_path": [VP, P(i32)],
     "ym_su3_measured_sweeps": [VP, f64, i32, i64, i64, P(f64)],
     "ym_reset_accounting": [VP],
     "ym_su3_reference_sweeps": [VP, f64, P(u64), i64, P(u64), P(u64)],

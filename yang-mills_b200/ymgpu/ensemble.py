@@ -144,6 +144,18 @@ class Ensemble:
                                            _f64p(out)), "su3_measured_sweeps")
         return out
 
+    @property
+    def sweep_path(self) -> str:
+        """'auto' (undecided), 'tiled' or 'resident' (include/ymgpu.h)."""
+        v = C.c_int32()
+        check(lib().ym_ensemble_get_sweep_path(self._h, C.byref(v)), "get_sweep_path")
+        return {-1: "auto", 0: "tiled", 1: "resident"}[v.value]
+
+    @sweep_path.setter
+    def sweep_path(self, value: str) -> None:
+        check(lib().ym_ensemble_set_sweep_path(self._h, {"auto": -1, "tiled": 0, "resident": 1}[value]),
+              "set_sweep_path")
+
     def accounting(self):
         p = np.zeros(self.n_chains, np.uint64)
         a = np.zeros(self.n_chains, np.uint64)
