@@ -122,30 +122,42 @@ def scalar_glueball_pipeline(groups: Sequence[Tuple[int, Sequence[int]]] = ((128
     res = GlueballPipelineResult()
     samples: Dict[Tuple[int, int, bool], List[Tuple[np.ndarray, np.ndarray]]] = {}
     with Ensemble(extents, beta, seeds, lift_reference_caps=True, device=device) as ens:
-        t0 = time.perf_counter()
-        ens.metropolis_sweeps(proposal_angle, thermalization)
-        ens.synchronize()
-        res.sweep_seconds += time.perf_counter() - t0
         per_group = [[i for i, g in enumerate(group_of) if g == gi] for gi in range(len(groups))]
-        for _ in range(measurements):
+        # Scratch handles made once and refilled every measurement: the
+        # smeared copy of all chains, and per blockable group its chains and
+        # their blocked lattices.
+        sm = ens.like()
+        subs, coarse = {}, {}
+        for gi, chains in enumerate(per_group):
+            if _blockable(groups[gi][1]):
+                subs[gi] = sm.subset(chains)
+                coarse[gi] = subs[gi].like([G.blocked_extents(e) for e in subs[gi].extents])
+        try:
             t0 = time.perf_counter()
-            ens.metropolis_sweeps(proposal_angle, sweeps_between_measurements)
+            ens.metropolis_sweeps(proposal_angle, thermalization)
             ens.synchronize()
-            t1 = time.perf_counter()
-            res.sweep_seconds += t1 - t0
-            for levels in stout_levels:
-                sm = G.spatial_stout_smear(ens, rho, levels, lift_level_cap=True)
-                basis = sm.scalar_operator_basis()
-                for gi, chains in enumerate(per_group):
-                    samples.setdefault((gi, levels, False), []).extend(basis[c] for c in chains)
-                    if _blockable(groups[gi][1]):
-                        sub = sm.subset(chains)
-                        co = G.spatial_stride2_block(sub)
-                        samples.setdefault((gi, levels, True), []).extend(co.scalar_operator_basis())
-                        co.close()
-                        sub.close()
-                sm.close()
-            res.measure_seconds += time.perf_counter() - t1
+            res.sweep_seconds += time.perf_counter() - t0
+            for _ in range(measurements):
+                t0 = time.perf_counter()
+                ens.metropolis_sweeps(proposal_angle, sweeps_between_measurements)
+                ens.synchronize()
+                t1 = time.perf_counter()
+                res.sweep_seconds += t1 - t0
+                for levels in stout_levels:
+                    ens.stout_smear_into(sm, rho, levels, lift_level_cap=True)
+                    basis = sm.scalar_operator_basis()
+                    for gi, chains in enumerate(per_group):
+                        samples.setdefault((gi, levels, False), []).extend(basis[c] for c in chains)
+                        if gi in subs:
+                            for j, c in enumerate(chains):
+                                sm.copy_chain_to(c, subs[gi], j)
+                            subs[gi].block_into(coarse[gi])
+                            samples.setdefault((gi, levels, True), []).extend(
+                                coarse[gi].scalar_operator_basis())
+                res.measure_seconds += time.perf_counter() - t1
+        finally:
+            for h in list(coarse.values()) + list(subs.values()) + [sm]:
+                h.close()
         res.link_updates = int(sum(np.prod(e) * 4 for e in extents)) * (
             thermalization + measurements * sweeps_between_measurements)
     for (gi, levels, blocked), rows in sorted(samples.items()):
