@@ -377,6 +377,66 @@ def main():
     sig = lambda a, b: abs(a["plaquette_mean"] - b["plaquette_mean"]) / np.hypot(
         a["plaquette_error"], b["plaquette_error"])
 
+    # the other configurations of the path, each short: throughput and
+    # plaquette ESS/s through the same estimator
+    def other_configs():
+        out = {}
+        from ymgpu.su2_ensemble import derive_chain_seed
+        # SU(2) 10^4 beta=2.3: 1 Kennedy-Pendleton heat-bath + 3 overrelaxation per sweep
+        e2 = ymgpu.Ensemble([[10, 10, 10, 10]], 2.3, derive_chain_seed(0x2B00201211160101, rank),
+                            group=ymgpu.SU2, device=local)
+        e2.set_identity()
+        e2.markov_sweeps(200, 3, sampler="kennedy-pendleton")
+        e2.synchronize()
+        series = np.zeros(500)
+        t = time.perf_counter()
+        for i in range(500):
+            e2.markov_sweeps(1, 3, sampler="kennedy-pendleton")
+            series[i] = e2.average_plaquette()[0]
+        secs = time.perf_counter() - t
+        e2.close()
+        d2 = diagnostics(series, 100)[0]
+        out["su2_10^4_beta2.3_kp+3or"] = {
+            "link_steps_per_s": world * 40000 * 4 * 500 / secs, "ms_per_sweep": 1e3 * secs / 500,
+            "plaquette_mean": float(series.mean()), "plaquette_ess_per_s": world * d2.effective_sample_size / secs,
+            "note": "200 + 500 sweeps from a cold start, plaquette every sweep (read back each sweep)"}
+        # SU(3) 64 x 4^4 beta=6.0 FP64, generator uniform in 1..8, half width 0.3
+        seeds = [derive_su3_chain_seed(MASTER_SEED, rank * 64 + i) for i in range(64)]
+        e1 = ymgpu.Ensemble([[4, 4, 4, 4]] * 64, BETA, seeds, device=local)
+        e1.metropolis_sweeps(1.0, 1000, "uniform")
+        e1.synchronize()
+        t = time.perf_counter()
+        s1 = e1.measured_sweeps(ANGLE, 1000, 1, "uniform")
+        secs = time.perf_counter() - t
+        path = e1.sweep_path
+        e1.close()
+        d1 = [diagnostics(s1[:, c], 100)[0] for c in range(64)]
+        m1 = s1.mean(0)
+        out["su3_64x4^4_fp64_uniform_0.3"] = {
+            "link_updates_per_s": world * 64 * 1024 * 1000 / secs, "us_per_sweep": 1e6 * secs / 1000,
+            "plaquette_ess_per_s": world * sum(d.effective_sample_size for d in d1) / secs,
+            "tau_int": float(np.mean([d.integrated_autocorrelation_time for d in d1])),
+            "plaquette_mean": float(m1.mean()), "plaquette_error": float(m1.std(ddof=1) / 8.0),
+            "sweep_path": path,
+            "note": "1000 measured sweeps (plaquette each) after 1000 at half width 1.0; one handle, "
+                    "graph-replayed or chain-resident as the handle's tuner chose"}
+        # scalar-glueball pipeline, batched uneven chains, beta=5.7
+        from ymgpu.pipelines import scalar_glueball_pipeline
+        t = time.perf_counter()
+        r = scalar_glueball_pipeline(thermalization=64, measurements=4, sweeps_between_measurements=4,
+                                     device=local)
+        secs = time.perf_counter() - t
+        out["glueball_pipeline_128x4^3x10+64x6^3x12+32x8^3x16"] = {
+            "seconds": secs, "sweep_seconds": r.sweep_seconds, "measure_seconds": r.measure_seconds,
+            "link_updates_per_s_in_sweeps": r.link_updates / r.sweep_seconds,
+            "surfaces": len(r.surfaces),
+            "note": "64 thermalisation sweeps, 4 measurements 4 sweeps apart; each measurement "
+                    "stout 0/5/10 levels (rho 0.1), stride-2 blocking of the 6^3 and 8^3 groups, "
+                    "A1++ operators; correlators, jackknife and covariance on the host"}
+        return out
+
+    configs_extra = other_configs()
+
     # end to end through the C ABI with host buffers: upload the lattice from
     # pinned host memory, sweep, measure, download the lattice
     host = torch.empty(links * 18, dtype=torch.float64, pin_memory=True)
@@ -436,6 +496,7 @@ def main():
                              "objective_last": float(np.mean(train_hist[-20:])),
                              "mean_half_width": float(np.mean(s_half)),
                              "mean_generator_probabilities": [float(v) for v in p_gen.mean(0)]}},
+            "other_configs": configs_extra,
             "ess": {
                 "geometry": f"{ESS_CHAINS} chains x 16^4 (total volume of 32^4), beta=6.0, "
                             f"{n} measured sweeps per sampler from one equilibrated state",
