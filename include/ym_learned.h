@@ -121,6 +121,14 @@ int32_t ym_su3_learned_measured_sweeps(ym_ensemble *ens, ym_proposal_model *mode
                                        int64_t n_measurements, int64_t sweeps_per_measurement,
                                        double *series);
 
+/* Failure detection of the tensor-core kernels: every wait for an MMA group
+ * gives up after a time limit, sets an error bit and returns, and the host
+ * reports YM_ERR_DEVICE_WAIT_TIMEOUT.  This runs that wait on a barrier that
+ * nothing completes, with limit_ns in [1e3, 1e9]; it returns
+ * YM_ERR_DEVICE_WAIT_TIMEOUT when the wait gave up as designed (and leaves
+ * the device usable), YM_OK would mean the wait did not run. */
+int32_t ym_device_wait_selftest(int32_t device, int64_t limit_ns);
+
 #ifdef __cplusplus
 }
 #endif

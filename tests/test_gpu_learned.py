@@ -6,8 +6,8 @@ Tolerances: the device network accumulates in FP32 where the oracle sums in
 binary64 over the same BF16-rounded operands, so an activation can land on
 the other side of a BF16 rounding boundary; outputs agree to 1e-5 (relative
 to max(1, |y|)) in at least 97% of rows and to 1e-2 in all, gradients to 3%
-of their norm, the objective to 1e-4 relative.  Features and M = U A come from binary32 staples: 2e-5 of their
-scale."""
+of their norm, the objective to 1e-4 relative.  Features and M = U A come
+from binary32 staples: 2e-5 of their scale."""
 import numpy as np
 import pytest
 
@@ -160,3 +160,19 @@ def test_trained_proposal_beats_plain():
     assert abs(m_l.mean() - m_p.mean()) <= 4 * err, (m_l.mean(), m_p.mean(), err)
     info = (t_l, t_p, s_half.mean(), p_gen.mean(0), hist[:3], hist[-3:])
     assert t_l < t_p / 1.5, info
+
+
+def test_bounded_wait_gives_up_and_device_stays_usable():
+    """Failure detection without a fault: the tensor-core kernels' bounded
+    wait, run on a barrier nothing completes, reports the timeout status and
+    the context keeps working."""
+    import time
+    import ymgpu
+    from ymgpu.errors import YmError
+    t = time.perf_counter()
+    code = ymgpu.lib().ym_device_wait_selftest(0, 2_000_000)   # 2 ms
+    assert code == 904 and time.perf_counter() - t < 5.0
+    assert ymgpu.lib().ym_device_wait_selftest(0, 10) != 0     # limit outside [1e3, 1e9] ns
+    with ymgpu.ProposalModel(seed=1) as model:
+        y = model.forward(np.zeros((5, 16), np.float32))
+    assert np.all(np.isfinite(y))

@@ -1132,6 +1132,20 @@ int64_t half_sites(const ym_ensemble *e) {
 
 extern "C" {
 
+int32_t ym_device_wait_selftest(int32_t device, int64_t limit_ns) {
+    if (limit_ns < 1000 || limit_ns > 1000000000) return YM_ERR_INVALID_ARGUMENT;
+    YM_CUDA(cudaSetDevice(device));
+    unsigned *d_err = nullptr;
+    YM_CUDA(dalloc(&d_err, 1));
+    unsigned bits = 0;
+    cudaError_t err = cudaMemset(d_err, 0, sizeof(unsigned));
+    if (err == cudaSuccess) err = ym::launch_lp_wait_selftest((uint64_t)limit_ns, d_err, nullptr);
+    if (err == cudaSuccess) err = cudaMemcpy(&bits, d_err, sizeof bits, cudaMemcpyDeviceToHost);
+    cudaFree(d_err);
+    YM_CUDA(err);
+    return bits ? YM_ERR_DEVICE_WAIT_TIMEOUT : YM_OK;
+}
+
 int32_t ym_model_create(int32_t device, uint64_t seed, double initial_scale, ym_proposal_model **out) {
     if (!out) return YM_ERR_NULL_ARGUMENT;
     *out = nullptr;

@@ -627,6 +627,16 @@ k_lp_sweep(const ChainInfo *__restrict__ chains, const Tile *__restrict__ tiles,
     teardown_block(tmem, 64);
 }
 
+// The tensor-core kernels' bounded mbarrier wait on a barrier that nothing
+// arrives on: it must give up after limit_ns and set the error bit.
+__global__ void k_lp_wait_selftest(uint64_t limit_ns, unsigned *err) {
+    __shared__ uint64_t mbar;
+    if (threadIdx.x == 0) umma::mbar_init(&mbar, 1);
+    __syncthreads();
+    const bool ok = umma::mbar_wait(&mbar, 0, limit_ns);
+    if (!ok && threadIdx.x == 0) atomicOr(err, kErrWait);
+}
+
 template <class K>
 cudaError_t allow_smem(K kernel, uint32_t bytes) {
     return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
@@ -635,6 +645,11 @@ cudaError_t allow_smem(K kernel, uint32_t bytes) {
 }  // namespace lp
 
 // ------------------------------------------------------------------ launchers
+
+cudaError_t launch_lp_wait_selftest(uint64_t limit_ns, unsigned *err, cudaStream_t st) {
+    lp::k_lp_wait_selftest<<<1, 32, 0, st>>>(limit_ns, err);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_lp_records(ym_ensemble *e, int parity, int mu, float *feat, float *m, float *b3) {
     if (e->n_half_tiles == 0) return cudaSuccess;

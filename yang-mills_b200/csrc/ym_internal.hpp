@@ -124,6 +124,7 @@ cudaError_t launch_lp_grad(ym_proposal_model *m, const float *feat, const float 
 cudaError_t launch_lp_adam(ym_proposal_model *m, int64_t n_tiles, int64_t n_valid, float lr,
                            int update, float *grad_out, double *objective_out, cudaStream_t st);
 cudaError_t launch_lp_sweep(ym_ensemble *e, ym_proposal_model *m, int parity, int mu);
+cudaError_t launch_lp_wait_selftest(uint64_t limit_ns, unsigned *err, cudaStream_t st);
 
 // Launchers implemented in su3_f64.cu (return a cudaError_t).
 cudaError_t launch_su3_identity(ym_ensemble *e);
