@@ -13,7 +13,8 @@ average-plaquette measurement.  The lattice (604 MB) is larger than the
 Beside it: the same steps with two-row binary32 links (``fp32_two_row``),
 with the learned proposal (``learned``: its network trained on the GPU on
 2000 configurations of the plain sampler), and the plaquette ESS/s of plain
-FP64, plain FP32 and learned FP32 sampling at the learned-proposal geometry
+FP64, plain FP32 (half width 0.3 and, as a control, the widest the
+reference admits, 1.0) and learned FP32 sampling at the learned-proposal geometry
 (16 chains of 16^4 in one handle, the total volume of 32^4), each judged by
 the reference's autocorrelation estimator (su2_ensemble.rs:375-463) on
 per-chain plaquette series.
@@ -46,7 +47,7 @@ ANGLE = 0.3
 THERMALIZATION = 1500                 # wide-angle sweeps from the hot start
 THERMALIZATION_ANGLE = 1.0            # the plaquette relaxes fastest at wide angles
 ESS_CHAINS, ESS_EXTENTS = 16, [16, 16, 16, 16]
-ESS_SWEEPS = 2000                     # measured sweeps per sampler (one plaquette each)
+ESS_SWEEPS = 3000                     # measured sweeps per sampler (one plaquette each)
 TRAIN_STEPS = 2000                    # configurations the plain sampler generates for training
 TRAIN_LR = 3e-3
 MASTER_SEED = 0x2C02198105010002
@@ -367,11 +368,14 @@ def main():
     e16.convert_to(e64)
     e32p = e16.like()
     e16.copy_to(e32p)
+    e32w = e16.like()
+    e16.copy_to(e32w)
     n = args.ess_sweeps
     ess_f64 = ess_leg(e64, lambda: e64.measured_sweeps(ANGLE, n, 1, "ordered"))
     ess_f32 = ess_leg(e32p, lambda: e32p.measured_sweeps(ANGLE, n, 1, "uniform"))
+    ess_f32w = ess_leg(e32w, lambda: e32w.measured_sweeps(1.0, n, 1, "uniform"))
     ess_lrn = ess_leg(e16, lambda: model.measured_sweeps(e16, n))
-    for e in (e64, e32p, e16):
+    for e in (e64, e32p, e32w, e16):
         e.close()
     model.close()
     sig = lambda a, b: abs(a["plaquette_mean"] - b["plaquette_mean"]) / np.hypot(
@@ -502,7 +506,11 @@ def main():
                             f"{n} measured sweeps per sampler from one equilibrated state",
                 "estimator": "reference diagnostics (initial positive window), per chain, summed",
                 "plain_f64_ordered_0.3": ess_f64, "plain_f32_uniform_0.3": ess_f32,
-                "learned_f32": ess_lrn,
+                "plain_f32_uniform_1.0": ess_f32w, "learned_f32": ess_lrn,
+                "control_note": "plain_f32_uniform_1.0 is plain Metropolis at the widest half "
+                                "width the reference admits",
+                "learned_vs_plain_f32_at_1.0": ess_lrn["plaquette_ess_per_s"] /
+                                               ess_f32w["plaquette_ess_per_s"],
                 "learned_vs_plain_f64": ess_lrn["plaquette_ess_per_s"] / ess_f64["plaquette_ess_per_s"],
                 "learned_vs_plain_f32": ess_lrn["plaquette_ess_per_s"] / ess_f32["plaquette_ess_per_s"],
                 "learned_vs_plain_f64_with_training": (

@@ -33,11 +33,18 @@
  * Outputs 0..7 are the generator logits, output 8 the scale, outputs 9..15
  * are padding kept at zero.
  *
- * Objective (training).  The expected squared jump of one hit,
- *   E = sum_a p_a * (1/2K) sum_{k, +-} alpha(dS_a(theta)) theta^2,
+ * Objective (training).  The expected squared change of the local action
+ * in one hit (the plaquette is the action, so this is the per-hit motion of
+ * the observable the sampler is judged on) plus an entropy term that keeps
+ * the generator logits near uniform unless a consistent gain moves them
+ * (E is linear in the probabilities, so without it gradient noise alone
+ * drifts the softmax onto one generator),
+ *   O = E + YM_LP_ENTROPY_WEIGHT * H(q),  H(q) = -sum_a q_a log q_a,
+ *   q = softmax(logits),
+ *   E = sum_a p_a * (1/2K) sum_{k, +-} alpha(dS_a(theta)) dS_a(theta)^2,
  *   theta = +-s (k + 1/2)/K, K = YM_LP_QUADRATURE,
  *   alpha = min(1, exp(-dS)),  dS_a(theta) = (beta/3)(ReTr M - ReTr(R_a(theta) M)),
- * M = U A, R_a(theta) = exp(i theta T^a); training maximises the mean of E
+ * M = U A, R_a(theta) = exp(i theta T^a); training maximises the mean of O
  * over the links of one checkerboard sub-sweep per configuration with Adam.
  */
 #ifndef YM_LEARNED_H
@@ -71,6 +78,7 @@ enum {
 #define YM_LP_SCALE_MIN 0.05
 #define YM_LP_SCALE_MAX 2.5
 #define YM_LP_GENERATOR_FLOOR 0.5
+#define YM_LP_ENTROPY_WEIGHT 0.02
 
 typedef struct ym_ensemble ym_ensemble;
 typedef struct ym_proposal_model ym_proposal_model;
@@ -92,7 +100,7 @@ int32_t ym_model_forward(ym_proposal_model *model, const float *features, int64_
                          float *outputs);
 /* Objective and gradient over host records, without an update:
  * features[n][16], m[n][18] (U A, row-major re/im), beta[n];
- * objective = mean E, grad[YM_LP_PARAMS] = d(-mean E)/d params. */
+ * objective = mean O, grad[YM_LP_PARAMS] = d(-mean O)/d params. */
 int32_t ym_model_gradient(ym_proposal_model *model, const float *features, const float *m,
                           const double *beta, int64_t n, double *objective, float *grad);
 

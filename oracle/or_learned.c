@@ -161,7 +161,7 @@ static void retr_rotated(int g, const mat3 *mm, double theta, double *f, double 
     }
 }
 
-/* E of one record and dE/dy for outputs 0..8. */
+/* Objective O = E + w H(q) of one record and dO/dy for outputs 0..8. */
 static double objective_row(const double y[16], const mat3 *m, double beta, double dy[9]) {
     double p[8], q[8], s, sig;
     proposal_q(y, q, p, &s, &sig);
@@ -176,11 +176,11 @@ static double objective_row(const double y[16], const mat3 *m, double beta, doub
             for (int sg = -1; sg <= 1; sg += 2) {
                 double dth = sg * gk, th = s * dth, f, df;
                 retr_rotated(a, m, th, &f, &df);
-                double ds = b3 * (tr - f);
+                double ds = b3 * (tr - f), dds = -b3 * df; /* dS and d dS / d theta */
                 double al = ds > 0.0 ? exp(-ds) : 1.0;
-                double dal = ds > 0.0 ? al * b3 * df : 0.0; /* d alpha / d theta */
-                j += al * th * th;
-                dj += (dal * th * th + 2.0 * al * th) * dth;
+                double dal = ds > 0.0 ? -al * dds : 0.0;   /* d alpha / d theta */
+                j += al * ds * ds;
+                dj += (dal * ds * ds + 2.0 * al * ds * dds) * dth;
             }
         }
         J[a] = j / (2.0 * K);
@@ -188,11 +188,16 @@ static double objective_row(const double y[16], const mat3 *m, double beta, doub
         E += p[a] * J[a];
         dEs += p[a] * dJ[a];
     }
-    double Eq = 0.0;
-    for (int a = 0; a < 8; ++a) Eq += q[a] * J[a];
-    for (int a = 0; a < 8; ++a) dy[a] = (1.0 - YM_LP_GENERATOR_FLOOR) * q[a] * (J[a] - Eq);
+    double Eq = 0.0, H = 0.0;
+    for (int a = 0; a < 8; ++a) {
+        Eq += q[a] * J[a];
+        H -= q[a] * log(q[a]);
+    }
+    for (int a = 0; a < 8; ++a)
+        dy[a] = (1.0 - YM_LP_GENERATOR_FLOOR) * q[a] * (J[a] - Eq) -
+                YM_LP_ENTROPY_WEIGHT * q[a] * (log(q[a]) + H);
     dy[8] = dEs * (YM_LP_SCALE_MAX - YM_LP_SCALE_MIN) * sig * (1.0 - sig);
-    return E;
+    return E + YM_LP_ENTROPY_WEIGHT * H;
 }
 
 int or_lp_retr_rotated(int g, const float *m18, double theta, double *f, double *df) {

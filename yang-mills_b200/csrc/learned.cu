@@ -227,7 +227,7 @@ __device__ __forceinline__ void retr_rotated(int g, const float *m, float tr, fl
     }
 }
 
-// Objective E of one record and dE/dy (outputs 0..8).
+// Objective O = E + w H(q) of one record and dO/dy (outputs 0..8).
 __device__ __forceinline__ float objective_row(const float y[16], const float *m, float b3, float dy[9]) {
     float mx = y[0];
 #pragma unroll
@@ -260,24 +260,28 @@ __device__ __forceinline__ float objective_row(const float y[16], const float *m
                 const float dth = sg * gk, th = s * dth;
                 float f, df;
                 retr_rotated(a, m, tr, th, f, df);
-                const float ds = b3 * (tr - f);
+                const float ds = b3 * (tr - f), dds = -b3 * df;
                 const float al = ds > 0.f ? expf(-ds) : 1.f;
-                const float dal = ds > 0.f ? al * b3 * df : 0.f;
-                j += al * th * th;
-                dj += (dal * th * th + 2.f * al * th) * dth;
+                const float dal = ds > 0.f ? -al * dds : 0.f;
+                j += al * ds * ds;
+                dj += (dal * ds * ds + 2.f * al * ds * dds) * dth;
             }
         }
         J[a] = j / (2.f * K);
         E += p[a] * J[a];
         dEs += p[a] * (dj / (2.f * K));
     }
-    float Eq = 0.f;
+    float Eq = 0.f, H = 0.f;
 #pragma unroll
-    for (int a = 0; a < 8; ++a) Eq += q[a] * J[a];
+    for (int a = 0; a < 8; ++a) {
+        Eq += q[a] * J[a];
+        H -= q[a] * logf(q[a]);
+    }
+    constexpr float W = (float)YM_LP_ENTROPY_WEIGHT;
 #pragma unroll
-    for (int a = 0; a < 8; ++a) dy[a] = (1.f - F) * q[a] * (J[a] - Eq);
+    for (int a = 0; a < 8; ++a) dy[a] = (1.f - F) * q[a] * (J[a] - Eq) - W * q[a] * (logf(q[a]) + H);
     dy[8] = dEs * (float)(YM_LP_SCALE_MAX - YM_LP_SCALE_MIN) * sig * (1.f - sig);
-    return E;
+    return E + W * H;
 }
 
 __device__ __forceinline__ void setup_block(uint8_t *sm, uint32_t slot_off, uint32_t mbar_off,

@@ -5,7 +5,7 @@ gauge-invariant features of a link's staple sum to eight generator logits
 and an angle scale (include/ym_learned.h has the exact definition).  It is
 trained on configurations the plain sampler generates, by the engine's own
 tensor-core forward and backward kernels, to maximise the expected squared
-jump of one hit; ``Ensemble`` chains in two-row binary32 storage are then
+change of the local action in one hit; ``Ensemble`` chains in two-row binary32 storage are then
 swept with it.  The proposal depends on the staple only, so it is symmetric
 and the exact accept/reject keeps detailed balance; plain Metropolis
 (``Ensemble.metropolis_sweeps``) stays the reference sampler it is judged
