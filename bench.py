@@ -347,6 +347,32 @@ def main():
     roofline.update({"traffic": ncu_traffic_per_launch(),
                      "kernel": "k_su3_metropolis (one checkerboard sub-sweep)"})
 
+    # spatial stout smearing of a 32^4 FP64 lattice (rho 0.1), each level
+    # timed by its CUDA-event pair; compulsory traffic per level: every link
+    # of every site read once and written once.  The reference's smearing
+    # checks every link against SU(3) to 5e-12, so the lattice is an FP64
+    # Haar hot start swept in FP64 (the thermalised one above came from
+    # binary32 storage).
+    src = ens.like()
+    src.hot_start()
+    src.metropolis_sweeps(1.0, 20, "uniform")
+    sm = src.like()
+    src.stout_smear_into(sm, 0.1, 1, lift_level_cap=True)
+    sm.profile(True)
+    src.stout_smear_into(sm, 0.1, 4, lift_level_cap=True)
+    st_ms, st_n = sm.profile_read("stout")
+    sm.profile(False)
+    sm.close()
+    src.close()
+    st_s = st_ms * 1e-3 / max(1, st_n)
+    st_bytes = volume * 8 * LINK_BYTES
+    stout = {"ms_per_level": st_s * 1e3, "levels_timed": st_n, "bytes_per_level": st_bytes,
+             "roofline": {"bound": "hbm", "achieved": st_bytes / st_s / 1e9, "peak": peak,
+                          "unit": "GB/s", "frac": st_bytes / st_s / 1e9 / peak,
+                          "peak_source": f"{peak_kind} hbm_gbs",
+                          "kernel": "k_stout_level (staples, Q, Cayley-Hamilton exponential "
+                                    "with the reference's checks, per spatial link)"}}
+
     # plaquette ESS/s of the three samplers at 16 x 16^4 from one equilibrated state
     def ess_leg(e, run):
         e.synchronize()
@@ -501,6 +527,7 @@ def main():
                              "mean_half_width": float(np.mean(s_half)),
                              "mean_generator_probabilities": [float(v) for v in p_gen.mean(0)]}},
             "other_configs": configs_extra,
+            "stout_32x4_fp64": stout,
             "ess": {
                 "geometry": f"{ESS_CHAINS} chains x 16^4 (total volume of 32^4), beta=6.0, "
                             f"{n} measured sweeps per sampler from one equilibrated state",
