@@ -105,6 +105,36 @@ typedef enum ym_status {
     YM_ERR_DEGENERATE_OBSERVABLE = 125,
     YM_ERR_NON_FINITE_RESULT = 126,
 
+    /* EffectiveMassError (glueball_effective_mass.rs:40-54; TimeExtentTooLarge,
+     * NonFiniteStatistic and AllocationFailed share the codes above),
+     * ScalarFitError (glueball_scalar_fit.rs:67-81; EffectiveMass(e) is e's
+     * code) and VariationalError (glueball_scalar_variational.rs:59-78;
+     * Operator(e) and Correlator(e) are e's code). */
+    YM_ERR_TIME_EXTENT_TOO_SMALL = 130,
+    YM_ERR_TOO_FEW_JACKKNIFE_REPLICATES = 131,
+    YM_ERR_TOO_MANY_JACKKNIFE_REPLICATES = 132,
+    YM_ERR_EMPTY_ANALYSIS_WINDOW = 133,
+    YM_ERR_INVALID_ANALYSIS_LAG = 134,
+    YM_ERR_SHAPE_MISMATCH = 135,
+    YM_ERR_NON_FINITE_CORRELATOR = 136,
+    YM_ERR_NON_POSITIVE_CENTRAL_CORRELATOR = 137,
+    YM_ERR_ACOSH_DOMAIN_VIOLATION = 138,
+    YM_ERR_INVALID_FIXTURE_PARAMETER = 139,
+    YM_ERR_EMPTY_CANDIDATE_WINDOWS = 140,
+    YM_ERR_TOO_MANY_CANDIDATE_WINDOWS = 141,
+    YM_ERR_DUPLICATE_CANDIDATE_WINDOW = 142,
+    YM_ERR_DEGENERATE_PLATEAU_UNCERTAINTY = 143,
+    YM_ERR_NO_ACCEPTED_PLATEAU_WINDOW = 144,
+    YM_ERR_COVARIANCE_NOT_POSITIVE_DEFINITE = 145,
+    YM_ERR_SINGULAR_COVARIANCE = 146,
+    YM_ERR_NO_FINITE_GRID_FIT = 147,
+    YM_ERR_MATRIX_NOT_SYMMETRIC = 150,
+    YM_ERR_INVALID_REFERENCE_TIMES = 151,
+    YM_ERR_REFERENCE_MATRIX_NOT_POSITIVE_DEFINITE = 152,
+    YM_ERR_DEGENERATE_PRINCIPAL_EIGENVECTOR = 153,
+    YM_ERR_NON_POSITIVE_PRINCIPAL_EIGENVALUE = 154,
+    YM_ERR_PROJECTION_NORMALIZATION_FAILURE = 155,
+
     /* Device boundary (no reference counterpart). */
     YM_ERR_NULL_ARGUMENT = 900,
     YM_ERR_INVALID_ARGUMENT = 901,

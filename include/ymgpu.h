@@ -33,6 +33,7 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#include "ym_analysis.h"
 #include "ym_learned.h"
 #include "ym_status.h"
 

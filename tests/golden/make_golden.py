@@ -25,6 +25,9 @@ FILES = [
     "glueball-spatial-stout-phase3b1-v1.json",
     "glueball-spatial-block-phase3b2-v1.json",
     "glueball-connected-correlator-phase3c-v1.json",
+    "glueball-effective-mass-phase3d-v1.json",
+    "glueball-scalar-fit-phase3e-v1.json",
+    "glueball-scalar-variational-phase3j-v1.json",
     "sampling-efficiency-v1.json",
     "su3-plaquette-baseline-v2.json",
     "su2-plaquette-baseline-v1.json",

@@ -76,11 +76,11 @@ __device__ __forceinline__ cplx det3(const m3 &m) {
     return cadd(csub(t1, t2), t3);
 }
 
-// Mat3::unitarity_residual (su3.rs:219-223): max |U^dag U - 1| and
-// |U U^dag - 1| over all entries.  Both products are Hermitian, so the
-// upper triangle (diagonal included) carries every distinct magnitude; only
-// those six entries of each are formed.
-__device__ __forceinline__ double unitarity_res(const m3 &u) {
+// Square of Mat3::unitarity_residual (su3.rs:219-223): max |U^dag U - 1|^2
+// and |U U^dag - 1|^2 over all entries.  Both products are Hermitian, so
+// the upper triangle (diagonal included) carries every distinct magnitude;
+// only those six entries of each are formed.
+__device__ __forceinline__ double unitarity_res2(const m3 &u) {
     double r = 0.0;
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
@@ -98,7 +98,7 @@ __device__ __forceinline__ double unitarity_res(const m3 &u) {
             r = fmax(r, fmax(norm2(l), norm2(g)));
         }
     }
-    return sqrt(r);
+    return r;
 }
 
 // Su3::from_checked_matrix gate (su3.rs:20, 241-252): finite, unitarity residual
@@ -106,7 +106,7 @@ __device__ __forceinline__ double unitarity_res(const m3 &u) {
 // which is the same number (det U^dag is the conjugate of det U).
 __device__ __forceinline__ bool in_su3(const m3 &u) {
     if (!finite3(u)) return false;
-    if (unitarity_res(u) > kSu3Tol) return false;
+    if (unitarity_res2(u) > kSu3Tol * kSu3Tol) return false;
     return norm2(csub(det3(u), cmake(1.0, 0.0))) <= kSu3Tol * kSu3Tol;
 }
 

@@ -105,6 +105,48 @@ SIGNATURES.update({
     "ym_sampling_efficiency": [P(f64), i64, P(f64), i64, f64, f64, f64, P(EfficiencyReport),
                                P(f64)],
 })
+
+
+# host analysis (include/ym_analysis.h)
+class EffectiveMassPoint(C.Structure):
+    _fields_ = [("tau", i64), ("full_estimate", f64), ("jackknife_mean", f64),
+                ("standard_error", f64)]
+
+
+class FitWindowC(C.Structure):
+    _fields_ = [("start", u64), ("end", u64)]
+
+
+class ScalarFitResultC(C.Structure):
+    _fields_ = [("time_extent", i64), ("jackknife_replicates", i64), ("selected_window", FitWindowC),
+                ("plateau_weighted_effective_mass", f64), ("plateau_maximum_z", f64),
+                ("fitted_mass", f64), ("fitted_amplitude", f64), ("chi_square", f64),
+                ("degrees_of_freedom", i64), ("chi_square_per_dof", f64),
+                ("mass_jackknife_mean", f64), ("mass_standard_error", f64),
+                ("amplitude_jackknife_mean", f64), ("amplitude_standard_error", f64),
+                ("maximum_off_diagonal_correlation", f64)]
+
+
+class PrincipalProjectionC(C.Structure):
+    _fields_ = [("reference_time", i64), ("diagonalization_time", i64),
+                ("principal_eigenvalue", f64), ("coefficients", f64 * 2)]
+
+
+SIGNATURES.update({
+    "ym_cosh_effective_mass_with_jackknife": [P(f64), i64, P(P(f64)), P(i64), i64, P(u64), i64,
+                                              P(EffectiveMassPoint)],
+    "ym_analytic_periodic_single_state": [i64, f64, f64, P(f64)],
+    "ym_correlated_scalar_fit": [P(f64), i64, P(P(f64)), P(i64), i64, P(FitWindowC), i64,
+                                 P(ScalarFitResultC)],
+    "ym_scalar_fit_window_covariance": [P(P(f64)), P(i64), i64, FitWindowC, P(f64)],
+    "ym_scalar_fit_invert_covariance": [P(f64), i64, P(f64)],
+    "ym_maximum_off_diagonal_correlation": [P(f64), i64, P(f64)],
+    "ym_canonical_scalar_fit_fixture": [P(f64), P(f64), P(FitWindowC)],
+    "ym_scalar_variational_connected_correlator": [P(f64), i64, i64, P(f64), P(f64)],
+    "ym_principal_generalized_projection": [P(f64), i64, i64, i64, P(PrincipalProjectionC), P(f64)],
+    "ym_canonical_two_state_matrices": [P(f64)],
+    "ym_max_matrix_series_residual": [P(f64), i64, P(f64), i64, P(f64)],
+})
 U64_FUNCTIONS = {
     "ym_derive_chain_seed": [u64, u64],
     "ym_derive_su3_chain_seed": [u64, u64],
