@@ -34,6 +34,7 @@
 #include <stdint.h>
 
 #include "ym_analysis.h"
+#include "ym_config.h"
 #include "ym_learned.h"
 #include "ym_status.h"
 

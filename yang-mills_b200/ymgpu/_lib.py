@@ -147,6 +147,13 @@ SIGNATURES.update({
     "ym_canonical_two_state_matrices": [P(f64)],
     "ym_max_matrix_series_residual": [P(f64), i64, P(f64), i64, P(f64)],
 })
+SIGNATURES.update({
+    # canonical configurations (include/ym_config.h)
+    "ym_su2_to_canonical_config": [P(i64), P(f64), i32, C.c_char_p, i64, P(i64)],
+    "ym_su2_from_canonical_config": [C.c_char_p, i64, i32, P(i64), P(f64), i64],
+    "ym_su3_to_canonical_config": [P(i64), P(f64), i32, C.c_char_p, i64, P(i64)],
+    "ym_su3_from_canonical_config": [C.c_char_p, i64, i32, P(i64), P(f64), i64],
+})
 U64_FUNCTIONS = {
     "ym_derive_chain_seed": [u64, u64],
     "ym_derive_su3_chain_seed": [u64, u64],
