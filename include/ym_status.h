@@ -135,6 +135,19 @@ typedef enum ym_status {
     YM_ERR_NON_POSITIVE_PRINCIPAL_EIGENVALUE = 154,
     YM_ERR_PROJECTION_NORMALIZATION_FAILURE = 155,
 
+    /* BenchmarkError (su2_benchmark.rs:56-66, su3_benchmark.rs:56-66; its
+     * NonFiniteStatistic is code 38). */
+    YM_ERR_WRONG_BENCHMARK_CONFIGURATION = 160,
+    YM_ERR_DUPLICATE_CHAIN_IDENTITY = 161,
+    YM_ERR_DUPLICATE_MEASUREMENT_SERIES = 162,
+    YM_ERR_INVALID_PLAQUETTE_SAMPLE = 163,
+    YM_ERR_INVALID_HEATBATH_ACCOUNTING = 164,
+    YM_ERR_INVALID_METROPOLIS_ACCOUNTING = 165,
+    YM_ERR_INVALID_ACCEPTANCE_EVIDENCE = 166,
+    YM_ERR_INVALID_LINK_UNIT_RESIDUAL = 167,
+    YM_ERR_INVALID_LINK_RESIDUAL = 168,
+    YM_ERR_STATIONARITY_DIAGNOSTIC_FAILED = 169,
+
     /* Device boundary (no reference counterpart). */
     YM_ERR_NULL_ARGUMENT = 900,
     YM_ERR_INVALID_ARGUMENT = 901,
