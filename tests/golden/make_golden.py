@@ -29,6 +29,7 @@ FILES = [
     "glueball-scalar-fit-phase3e-v1.json",
     "glueball-scalar-variational-phase3j-v1.json",
     "sampling-efficiency-v1.json",
+    "su3-plaquette-baseline-v1.json",
     "su3-plaquette-baseline-v2.json",
     "su2-plaquette-baseline-v1.json",
 ]

@@ -56,7 +56,7 @@ void free_all(ym_ensemble *e) {
             cudaEventDestroy(p.start);
             cudaEventDestroy(p.stop);
         }
-    void *ptrs[] = {e->d_chains, e->d_half_tiles, e->d_site_tiles, e->d_site_tile_first,
+    void *ptrs[] = {e->d_chains, e->d_half_tiles, e->d_site_tiles, e->d_mixed_tiles, e->d_site_tile_first,
                     e->d_links, e->d_staging, e->d_partial, e->d_partial2, e->d_result,
                     e->d_result2, e->d_accepts, e->d_sweep, e->d_rng, e->d_ref_counts,
                     e->d_error, e->d_obs_partial, e->d_obs_out, e->d_site_vals,
@@ -295,6 +295,20 @@ int32_t ym_ensemble_create(const ym_ensemble_desc *desc, ym_ensemble **out) {
         for (int64_t s = 0; s < c.volume; s += ym::kSiteThreads) site.push_back(Tile{(int32_t)ch, 0, s});
     }
     first.push_back((int32_t)site.size());
+    // even tile k of a chain next to its odd tile k, so both parities of a
+    // region are in flight (and in L2) together
+    std::vector<Tile> mixed;
+    mixed.reserve(site.size());
+    for (int64_t ch = 0; ch < e->n_chains; ++ch) {
+        const ChainInfo &c = e->chains[ch];
+        std::vector<Tile> ev, od;
+        for (int32_t t = first[(size_t)ch]; t < first[(size_t)ch + 1]; ++t)
+            (site[(size_t)t].start < c.half || !c.eo ? ev : od).push_back(site[(size_t)t]);
+        for (size_t k = 0; k < ev.size() || k < od.size(); ++k) {
+            if (k < ev.size()) mixed.push_back(ev[k]);
+            if (k < od.size()) mixed.push_back(od[k]);
+        }
+    }
     e->n_half_tiles = (int64_t)half.size();
     e->n_site_tiles = (int64_t)site.size();
 
@@ -303,6 +317,7 @@ int32_t ym_ensemble_create(const ym_ensemble_desc *desc, ym_ensemble **out) {
     if (err == cudaSuccess) err = dalloc(&e->d_chains, e->chains.size());
     if (err == cudaSuccess) err = dalloc(&e->d_half_tiles, half.size());
     if (err == cudaSuccess) err = dalloc(&e->d_site_tiles, site.size());
+    if (err == cudaSuccess) err = dalloc(&e->d_mixed_tiles, mixed.size());
     if (err == cudaSuccess) err = dalloc(&e->d_site_tile_first, first.size());
     if (err == cudaSuccess) err = dalloc(&e->d_links, (size_t)e->total_elems);
     if (err == cudaSuccess) err = dalloc(&e->d_staging, (size_t)e->max_chain_links * 18);
@@ -322,6 +337,8 @@ int32_t ym_ensemble_create(const ym_ensemble_desc *desc, ym_ensemble **out) {
         err = cudaMemcpy(e->d_half_tiles, half.data(), half.size() * sizeof(Tile), cudaMemcpyHostToDevice);
     if (err == cudaSuccess && !site.empty())
         err = cudaMemcpy(e->d_site_tiles, site.data(), site.size() * sizeof(Tile), cudaMemcpyHostToDevice);
+    if (err == cudaSuccess && !mixed.empty())
+        err = cudaMemcpy(e->d_mixed_tiles, mixed.data(), mixed.size() * sizeof(Tile), cudaMemcpyHostToDevice);
     if (err == cudaSuccess)
         err = cudaMemcpy(e->d_site_tile_first, first.data(), first.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
     if (err == cudaSuccess) err = cudaMemset(e->d_accepts, 0, (size_t)e->n_chains * sizeof(unsigned long long));

@@ -212,7 +212,7 @@ k_stout_level(const ChainInfo *__restrict__ chains, const Tile *__restrict__ til
 }  // namespace
 
 cudaError_t launch_stout_level(ym_ensemble *e, const double2 *in, double2 *out, double rho) {
-    k_stout_level<<<(unsigned)e->n_site_tiles, T, 0, e->stream>>>(e->d_chains, e->d_site_tiles, in, out,
+    k_stout_level<<<(unsigned)e->n_site_tiles, T, 0, e->stream>>>(e->d_chains, e->d_mixed_tiles, in, out,
                                                                  rho, e->d_error);
     return cudaGetLastError();
 }

@@ -35,6 +35,9 @@ struct ym_ensemble {
     ym::Tile *d_half_tiles = nullptr;      // work items = checkerboard half
     int64_t n_half_tiles = 0;
     ym::Tile *d_site_tiles = nullptr;      // work items = all sites
+    ym::Tile *d_mixed_tiles = nullptr;     // the same tiles, each chain's even and odd halves
+                                           // interleaved (order-free per-site kernels whose
+                                           // neighbours are the other parity: stout smearing)
     int64_t n_site_tiles = 0;
     int32_t *d_site_tile_first = nullptr;  // first site tile of each chain (+ end)
 
