@@ -463,6 +463,35 @@ def main():
             "note": "64 thermalisation sweeps, 4 measurements 4 sweeps apart; each measurement "
                     "stout 0/5/10 levels (rho 0.1), stride-2 blocking of the 6^3 and 8^3 groups, "
                     "A1++ operators; correlators, jackknife and covariance on the host"}
+        # the reference's phase-3F production campaign (16 x 4^3x10, beta 5.7) with
+        # its correlated fits, and the published-baseline acceptance harnesses
+        from ymgpu import benchmarks as B
+        from ymgpu import production as P
+        t = time.perf_counter()
+        ps = P.run_production_scalar_analysis(device=local)
+        out["glueball_production_phase3f_16x4^3x10"] = {
+            "seconds": time.perf_counter() - t,
+            "surface_outcomes": [f"{r.outcome.transformation}/{r.outcome.operator}: "
+                                 + ("fit m=%.4f+-%.4f" % (r.outcome.fit.fitted_mass,
+                                                          r.outcome.fit.mass_standard_error)
+                                    if r.outcome.fit else r.outcome.error_code)
+                                 for r in ps.surfaces],
+            "scalar_pipeline_validated": ps.scalar_pipeline_validated,
+            "matches_reference_observed_receipt": P.observed_phase3f_receipt_matches(ps),
+            "note": "64 + 4 sweeps per chain on the device, stout 0/1/2, A1++ operators; "
+                    "correlators, jackknife and the correlated fits on the host"}
+        harness = {}
+        for name, fn, gate in (("su2_10^4_phase2b", B.run_su2_benchmark, "phase2_graduation_gate_satisfied"),
+                               ("su3_4^4_phase2c2_v1", B.run_su3_benchmark, "published_su3_baseline_reproduced"),
+                               ("su3_4^4_confirmation_v2", B.run_su3_confirmation,
+                                "published_su3_baseline_reproduced")):
+            t = time.perf_counter()
+            s = fn(device=local)
+            harness[name] = {"seconds": time.perf_counter() - t, "pooled_mean": s.pooled_mean,
+                             "pooled_standard_error": s.pooled_standard_error,
+                             "source_envelope_reproduced": s.source_envelope_reproduced,
+                             "diagnostics_trustworthy": s.diagnostics_trustworthy, gate: getattr(s, gate)}
+        out["published_baseline_harnesses"] = harness
         return out
 
     configs_extra = other_configs()

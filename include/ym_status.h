@@ -148,6 +148,11 @@ typedef enum ym_status {
     YM_ERR_INVALID_LINK_RESIDUAL = 168,
     YM_ERR_STATIONARITY_DIAGNOSTIC_FAILED = 169,
 
+    /* ProductionError (glueball_scalar_production.rs:159-172; its other
+     * variants share the codes above or wrap an inner variant). */
+    YM_ERR_CORRELATOR_REPLAY_MISMATCH = 170,
+    YM_ERR_LINK_RESIDUAL_EXCEEDED = 171,
+
     /* Device boundary (no reference counterpart). */
     YM_ERR_NULL_ARGUMENT = 900,
     YM_ERR_INVALID_ARGUMENT = 901,

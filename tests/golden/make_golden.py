@@ -28,6 +28,7 @@ FILES = [
     "glueball-effective-mass-phase3d-v1.json",
     "glueball-scalar-fit-phase3e-v1.json",
     "glueball-scalar-variational-phase3j-v1.json",
+    "glueball-scalar-production-phase3f-v1.json",
     "sampling-efficiency-v1.json",
     "su3-plaquette-baseline-v1.json",
     "su3-plaquette-baseline-v2.json",
