@@ -467,19 +467,27 @@ def main():
         # its correlated fits, and the published-baseline acceptance harnesses
         from ymgpu import benchmarks as B
         from ymgpu import production as P
-        t = time.perf_counter()
-        ps = P.run_production_scalar_analysis(device=local)
-        out["glueball_production_phase3f_16x4^3x10"] = {
-            "seconds": time.perf_counter() - t,
-            "surface_outcomes": [f"{r.outcome.transformation}/{r.outcome.operator}: "
-                                 + ("fit m=%.4f+-%.4f" % (r.outcome.fit.fitted_mass,
-                                                          r.outcome.fit.mass_standard_error)
-                                    if r.outcome.fit else r.outcome.error_code)
-                                 for r in ps.surfaces],
-            "scalar_pipeline_validated": ps.scalar_pipeline_validated,
-            "matches_reference_observed_receipt": P.observed_phase3f_receipt_matches(ps),
-            "note": "64 + 4 sweeps per chain on the device, stout 0/1/2, A1++ operators; "
-                    "correlators, jackknife and the correlated fits on the host"}
+        campaigns = {}
+        for name, c in P.CAMPAIGNS.items():
+            t = time.perf_counter()
+            ps = P.run_campaign(c, device=local)
+            secs = time.perf_counter() - t
+            total = c.expected_proposals_per_chain * c.chain_count
+            campaigns[name] = {
+                "chains": f"{c.chain_count} x {'x'.join(map(str, c.extents))}", "seconds": secs,
+                "proposals": total, "proposals_per_s": total / secs,
+                "surface_outcomes": [f"{r.outcome.transformation}/{r.outcome.operator}: "
+                                     + ("fit m=%.4f+-%.4f" % (r.outcome.fit.fitted_mass,
+                                                              r.outcome.fit.mass_standard_error)
+                                        if r.outcome.fit else r.outcome.error_code)
+                                     for r in ps.surfaces],
+                "scalar_pipeline_validated": ps.scalar_pipeline_validated,
+                "matches_reference_observed_receipt": (P.observed_receipt_matches(ps, c)
+                                                       if c.observed_outcomes else "no receipt recorded")}
+        campaigns["note"] = ("each campaign: 64 + 4 sweeps per chain on the device, stout 0/1/2 "
+                             "(and stride-2 blocking for 3H/3I), A1++ operators; correlators, "
+                             "jackknife and the correlated fits on the host; seconds include all of it")
+        out["glueball_production_campaigns"] = campaigns
         harness = {}
         for name, fn, gate in (("su2_10^4_phase2b", B.run_su2_benchmark, "phase2_graduation_gate_satisfied"),
                                ("su3_4^4_phase2c2_v1", B.run_su3_benchmark, "published_su3_baseline_reproduced"),

@@ -32,3 +32,21 @@ def test_production_campaign_on_device(oracle):
     again = P.summarize_surfaces(s.chain_evidence, s.surfaces)
     assert again.scalar_pipeline_validated == s.scalar_pipeline_validated
     assert again.primary_window_successes == s.primary_window_successes
+
+
+def test_recovery_campaigns_reproduce_the_recorded_receipts():
+    """Phases 3G and 3H (glueball_scalar_recovery_receipt.rs,
+    glueball_scalar_geometry_recovery_receipt.rs) recorded all surfaces
+    rejected on the effective mass; phase 3I has no recorded outcome and
+    runs to a complete summary (2.4e8 proposals)."""
+    from ymgpu import production as P
+    for name in ("phase3g", "phase3h"):
+        c = P.CAMPAIGNS[name]
+        s = P.run_campaign(c)
+        assert P.observed_receipt_matches(s, c), name
+    c = P.CAMPAIGNS["phase3i"]
+    s = P.run_campaign(c)
+    assert c.expected_proposals_per_chain * c.chain_count == 240_648_192
+    assert s.sampler_diagnostics_passed and len(s.surfaces) == 8
+    assert [(r.outcome.transformation, r.outcome.operator) for r in s.surfaces] == \
+        [(t, o) for t, _, _ in c.transformations for o in P.OPERATORS]
