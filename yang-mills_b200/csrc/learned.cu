@@ -583,9 +583,14 @@ __global__ void k_lp_adam(const double *__restrict__ groups, int64_t n_groups, i
 }
 
 // The learned sub-sweep (parity, MU) of a two-row ensemble.
+// Persistent: each CTA allocates its tensor memory, initialises its barrier
+// and stages the weight image once, then walks the tiles blockIdx.x,
+// blockIdx.x + gridDim.x, ...  Every tile's three MMA groups are waited for
+// before its hits, so the shared-memory operand tiles and the accumulator
+// columns are free again when the next tile writes them.
 template <int MU>
 __global__ void __launch_bounds__(kRows, 4)
-k_lp_sweep(const ChainInfo *__restrict__ chains, const Tile *__restrict__ tiles,
+k_lp_sweep(const ChainInfo *__restrict__ chains, const Tile *__restrict__ tiles, int64_t n_tiles,
            float2 *__restrict__ links, int parity, const uint4 *__restrict__ image,
            const float *__restrict__ params, const uint64_t *__restrict__ sweep_ptr,
            unsigned long long *__restrict__ accepts, unsigned *err) {
@@ -594,40 +599,46 @@ k_lp_sweep(const ChainInfo *__restrict__ chains, const Tile *__restrict__ tiles,
     extern __shared__ __align__(1024) uint8_t sm[];
     setup_block(sm, L::SLOT, L::MBAR, 64);
     stage_weights(sm, image, params, reinterpret_cast<float *>(sm + L::BIAS));
-    const Tile tile = tiles[blockIdx.x];
-    const ChainInfo c = chains[tile.chain];
-    const int64_t t = tile.start + threadIdx.x;
-    const bool valid = t < c.half;
-    const int64_t s = (int64_t)parity * c.half + (valid ? t : 0);
-    const Coord x = decode_storage(c, s);
-    m3f a;
-    float f[16];
-    if (valid) {
-        a = staple_f<MU>(links, c, x, parity);
-        staple_features(a, (float)c.beta, f);
-    } else {
-#pragma unroll
-        for (int i = 0; i < 16; ++i) f[i] = 0.f;
-    }
-    write_x_row(sm + L::X, threadIdx.x, f);
-    sync_for_mma();
-    const uint32_t tmem = *reinterpret_cast<volatile uint32_t *>(sm + L::SLOT);
     uint64_t *mbar = reinterpret_cast<uint64_t *>(sm + L::MBAR);
     uint32_t phase = 0;
-    float y[16];
-    const bool ok = forward_tile<L>(sm, tmem, mbar, phase, 0, 0, 0, err, y);
-    unsigned accepted = 0;
-    if (ok && valid) {
-        float cum[7], scale;
-        proposal_from(y, cum, scale);
-        m3f u = load_f(links, c, s, MU);
-        const uint64_t key = link_key(c.seed, *sweep_ptr, x.lex, MU);
-        accepted = visit_learned_f(u, a, c.beta / 3.0, cum, scale, key);
-        store_f(links, c, s, MU, u);
+    uint32_t tmem = 0;
+    const uint64_t sweep = *sweep_ptr;
+    for (int64_t ti = blockIdx.x; ti < n_tiles; ti += gridDim.x) {
+        const Tile tile = tiles[ti];
+        const ChainInfo c = chains[tile.chain];
+        const int64_t t = tile.start + threadIdx.x;
+        const bool valid = t < c.half;
+        const int64_t s = (int64_t)parity * c.half + (valid ? t : 0);
+        const Coord x = decode_storage(c, s);
+        m3f a;
+        float f[16];
+        if (valid) {
+            a = staple_f<MU>(links, c, x, parity);
+            staple_features(a, (float)c.beta, f);
+        } else {
+#pragma unroll
+            for (int i = 0; i < 16; ++i) f[i] = 0.f;
+        }
+        write_x_row(sm + L::X, threadIdx.x, f);
+        sync_for_mma();
+        tmem = *reinterpret_cast<volatile uint32_t *>(sm + L::SLOT);
+        float y[16];
+        const bool ok = forward_tile<L>(sm, tmem, mbar, phase, 0, 0, 0, err, y);
+        if (!ok) break;   // block-uniform: the wait gave up and set the error bit
+        unsigned accepted = 0;
+        if (valid) {
+            float cum[7], scale;
+            proposal_from(y, cum, scale);
+            m3f u = load_f(links, c, s, MU);
+            const uint64_t key = link_key(c.seed, sweep, x.lex, MU);
+            accepted = visit_learned_f(u, a, c.beta / 3.0, cum, scale, key);
+            store_f(links, c, s, MU, u);
+        }
+        const unsigned warp_sum = __reduce_add_sync(0xffffffffu, accepted);
+        if ((threadIdx.x & 31) == 0 && warp_sum)
+            atomicAdd(accepts + tile.chain, (unsigned long long)warp_sum);
     }
-    const unsigned warp_sum = __reduce_add_sync(0xffffffffu, accepted);
-    if ((threadIdx.x & 31) == 0 && warp_sum)
-        atomicAdd(accepts + tile.chain, (unsigned long long)warp_sum);
+    if (tmem == 0) tmem = *reinterpret_cast<volatile uint32_t *>(sm + L::SLOT);
     teardown_block(tmem, 64);
 }
 
@@ -734,15 +745,23 @@ cudaError_t launch_lp_sweep(ym_ensemble *e, ym_proposal_model *m, int parity, in
         configured_device = dev;
     }
     if (e->n_half_tiles == 0) return cudaSuccess;
-    const dim3 grid((unsigned)e->n_half_tiles);
+    static thread_local int resident_ctas = 0, resident_device = -1;
+    if (resident_device != dev) {   // 4 CTAs per SM: registers, shared memory and 4 x 64 TMEM columns
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        resident_ctas = 4 * sms;
+        resident_device = dev;
+    }
+    const int64_t n = e->n_half_tiles;
+    const dim3 grid((unsigned)(n < resident_ctas ? n : resident_ctas));
     float2 *links = reinterpret_cast<float2 *>(e->d_links);
     const uint4 *img = reinterpret_cast<const uint4 *>(m->d_image);
     const uint32_t sm = lp::FwdLayout::BYTES;
     switch (mu) {
-        case 0: lp::k_lp_sweep<0><<<grid, lp::kRows, sm, e->stream>>>(e->d_chains, e->d_half_tiles, links, parity, img, m->d_params, e->d_sweep, e->d_accepts, m->d_error); break;
-        case 1: lp::k_lp_sweep<1><<<grid, lp::kRows, sm, e->stream>>>(e->d_chains, e->d_half_tiles, links, parity, img, m->d_params, e->d_sweep, e->d_accepts, m->d_error); break;
-        case 2: lp::k_lp_sweep<2><<<grid, lp::kRows, sm, e->stream>>>(e->d_chains, e->d_half_tiles, links, parity, img, m->d_params, e->d_sweep, e->d_accepts, m->d_error); break;
-        default: lp::k_lp_sweep<3><<<grid, lp::kRows, sm, e->stream>>>(e->d_chains, e->d_half_tiles, links, parity, img, m->d_params, e->d_sweep, e->d_accepts, m->d_error); break;
+        case 0: lp::k_lp_sweep<0><<<grid, lp::kRows, sm, e->stream>>>(e->d_chains, e->d_half_tiles, n, links, parity, img, m->d_params, e->d_sweep, e->d_accepts, m->d_error); break;
+        case 1: lp::k_lp_sweep<1><<<grid, lp::kRows, sm, e->stream>>>(e->d_chains, e->d_half_tiles, n, links, parity, img, m->d_params, e->d_sweep, e->d_accepts, m->d_error); break;
+        case 2: lp::k_lp_sweep<2><<<grid, lp::kRows, sm, e->stream>>>(e->d_chains, e->d_half_tiles, n, links, parity, img, m->d_params, e->d_sweep, e->d_accepts, m->d_error); break;
+        default: lp::k_lp_sweep<3><<<grid, lp::kRows, sm, e->stream>>>(e->d_chains, e->d_half_tiles, n, links, parity, img, m->d_params, e->d_sweep, e->d_accepts, m->d_error); break;
     }
     return cudaGetLastError();
 }
