@@ -232,32 +232,20 @@ def main():
     rank, world, local = dist_env()
     import numpy as np
     import torch
-    import torch.distributed as dist
     import ymgpu
+    from ymgpu.replicas import Replicas
     from ymgpu.su2_ensemble import diagnostics
     from ymgpu.su3_ensemble import derive_su3_chain_seed
 
     torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    seed = derive_su3_chain_seed(MASTER_SEED, rank)
+    # one process per GPU, replicas only: barrier, slowest-rank timing, rank-0 output
+    rep = Replicas(backend="nccl", timeout_s=120, device=torch.device("cuda", local))
+    barrier = rep.barrier
+    max_over_ranks = rep.max_over_ranks
+    seed = rep.chain_seed(MASTER_SEED)
     volume = int(np.prod(EXTENTS))
     links = 4 * volume
     peak, peak_kind = measured_peaks()
-
-    def max_over_ranks(x):
-        if world > 1:
-            t = torch.tensor([x], device=f"cuda:{local}")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            return float(t.item())
-        return x
 
     def timed_leg(ens, step, link_bytes, kernel, sampler_clocks=False):
         """W warm-up steps, then args.steps steps (step() = one sweep) each
@@ -584,9 +572,8 @@ def main():
                 "plaquette_sigma_learned_vs_f64": float(sig(ess_lrn, ess_f64)),
                 "plaquette_sigma_f32_vs_f64": float(sig(ess_f32, ess_f64))},
         }
-        print(json.dumps(line))
-    if world > 1:
-        dist.destroy_process_group()
+        rep.emit(line)
+    rep.close()
 
 
 if __name__ == "__main__":
