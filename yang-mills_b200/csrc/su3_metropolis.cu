@@ -19,7 +19,9 @@
 //
 // Layout: per thread the staple accumulator lives in shared memory (18
 // doubles per thread, conflict-free column layout) so the register budget
-// holds three matrices at most and four 128-thread blocks fit per SM.
+// holds three matrices at most and four 128-thread blocks fit per SM.  The
+// third factor of every staple term is copied global -> shared by cp.async
+// when the term starts, so its latency overlaps the first product.
 #include <cuda_runtime.h>
 
 #include "su3_exp.cuh"
@@ -50,17 +52,48 @@ __device__ __forceinline__ void sa_col(const double (*sa)[T], int i, cplx col[3]
     for (int k = 0; k < 3; ++k) col[k] = sa_get(sa, 3 * k + i);
 }
 
+// Asynchronous 16-byte global -> shared copies (cp.async, L2 only): the
+// third factor of a staple term is fetched while the first product of the
+// term is computed, without holding registers for it.
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// Link (s, mu) into this thread's column of the staging buffer.
+__device__ __forceinline__ void stage_link(double2 (*buf)[T], const double2 *links, const ChainInfo &c,
+                                           int64_t s, int mu) {
+    const double2 *p = links + c.offset + (int64_t)(mu * 9) * c.volume + s;
+#pragma unroll
+    for (int e = 0; e < 9; ++e) cp_async16(&buf[e][threadIdx.x], p + (int64_t)e * c.volume);
+    cp_async_commit();
+}
+
+__device__ __forceinline__ m3 staged_link(const double2 (*buf)[T]) {
+    m3 o;
+#pragma unroll
+    for (int e = 0; e < 9; ++e) {
+        const double2 v = buf[e][threadIdx.x];
+        o.e[e / 3][e % 3] = cmake(v.x, v.y);
+    }
+    return o;
+}
+
 // The two staple terms of direction NU for link (x, MU):
 //   forward  U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag
 //   backward U_nu(x-nu+mu)^dag U_mu(x-nu)^dag U_nu(x-nu)
 // P = first two factors (fma chains from zero), then A += P * third factor.
 template <int MU, int NU, bool RESIDENT = false>
 __device__ __forceinline__ void add_staple(const double2 *__restrict__ links, const ChainInfo &c,
-                                           const Coord &x, int par, const Nb &pm, double (*sa)[T]) {
+                                           const Coord &x, int par, const Nb &pm, double (*sa)[T],
+                                           double2 (*buf)[T]) {
     const Nb pn = step(c, x.x, x.lex, par, NU, +1);
     const Nb mn = step(c, x.x, x.lex, par, NU, -1);
     const Nb mnpm = step(c, x.x, mn.lex, mn.par, MU, +1);   // x-nu keeps x's mu coordinate
     {
+        stage_link(buf, links, c, storage_index(c, x.lex, par), NU);
         const m3 l2 = link_at<RESIDENT>(links, c, storage_index(c, pn.lex, pn.par), MU);
         const m3 l1 = link_at<RESIDENT>(links, c, storage_index(c, pm.lex, pm.par), NU);
         m3 p;
@@ -73,7 +106,8 @@ __device__ __forceinline__ void add_staple(const double2 *__restrict__ links, co
                 for (int j = 0; j < 3; ++j) cfma(v, l1.e[r][j], cconj(l2.e[k][j]));
                 p.e[r][k] = v;
             }
-        const m3 l3 = link_at<RESIDENT>(links, c, storage_index(c, x.lex, par), NU);
+        cp_async_wait_all();
+        const m3 l3 = staged_link(buf);
 #pragma unroll
         for (int r = 0; r < 3; ++r)
 #pragma unroll
@@ -85,6 +119,7 @@ __device__ __forceinline__ void add_staple(const double2 *__restrict__ links, co
             }
     }
     {
+        stage_link(buf, links, c, storage_index(c, mn.lex, mn.par), NU);
         const m3 l2 = link_at<RESIDENT>(links, c, storage_index(c, mn.lex, mn.par), MU);
         const m3 l1 = link_at<RESIDENT>(links, c, storage_index(c, mnpm.lex, mnpm.par), NU);
         m3 p;
@@ -97,7 +132,8 @@ __device__ __forceinline__ void add_staple(const double2 *__restrict__ links, co
                 for (int j = 0; j < 3; ++j) cfma(v, cconj(l1.e[j][r]), cconj(l2.e[k][j]));
                 p.e[r][k] = v;
             }
-        const m3 l3 = link_at<RESIDENT>(links, c, storage_index(c, mn.lex, mn.par), NU);
+        cp_async_wait_all();
+        const m3 l3 = staged_link(buf);
 #pragma unroll
         for (int r = 0; r < 3; ++r)
 #pragma unroll
@@ -283,6 +319,7 @@ k_su3_metropolis(const ChainInfo *__restrict__ chains, const Tile *__restrict__ 
                  double2 *__restrict__ links, int parity, double angle, int uniform,
                  const uint64_t *__restrict__ sweep_ptr, unsigned long long *__restrict__ accepts) {
     __shared__ double sa[18][T];
+    __shared__ double2 l3buf[9][T];
     const Tile tile = tiles[blockIdx.x];
     const ChainInfo c = chains[tile.chain];
     const int64_t t = tile.start + threadIdx.x;
@@ -293,10 +330,10 @@ k_su3_metropolis(const ChainInfo *__restrict__ chains, const Tile *__restrict__ 
 #pragma unroll
         for (int e = 0; e < 18; ++e) sa[e][threadIdx.x] = 0.0;
         const Nb pm = step(c, x.x, x.lex, parity, MU, +1);
-        if (MU != 0) add_staple<MU, 0>(links, c, x, parity, pm, sa);
-        if (MU != 1) add_staple<MU, 1>(links, c, x, parity, pm, sa);
-        if (MU != 2) add_staple<MU, 2>(links, c, x, parity, pm, sa);
-        if (MU != 3) add_staple<MU, 3>(links, c, x, parity, pm, sa);
+        if (MU != 0) add_staple<MU, 0>(links, c, x, parity, pm, sa, l3buf);
+        if (MU != 1) add_staple<MU, 1>(links, c, x, parity, pm, sa, l3buf);
+        if (MU != 2) add_staple<MU, 2>(links, c, x, parity, pm, sa, l3buf);
+        if (MU != 3) add_staple<MU, 3>(links, c, x, parity, pm, sa, l3buf);
         m3 u = load_su3_rw(links, c, s, MU);
         const uint64_t key = link_key(c.seed, *sweep_ptr, x.lex, MU);
         accepted = visit(u, sa, c.beta / 3.0, angle, key, uniform);
