@@ -18,10 +18,11 @@
 //     bit.
 //
 // Layout: per thread the staple accumulator lives in shared memory (18
-// doubles per thread, conflict-free column layout) so the register budget
-// holds three matrices at most and four 128-thread blocks fit per SM.  The
-// third factor of every staple term is copied global -> shared by cp.async
-// when the term starts, so its latency overlaps the first product.
+// doubles per thread, conflict-free column layout), and every factor of the
+// six staple terms is copied global -> shared by cp.async ahead of its use
+// (the first two factors one term ahead, the third when its term starts), so
+// loads overlap the products without holding registers; three 128-thread
+// blocks fit per SM.
 #include <cuda_runtime.h>
 
 #include "su3_exp.cuh"
@@ -29,7 +30,10 @@
 #include "ym_internal.hpp"
 
 #ifndef YM_METRO_MIN_BLOCKS
-#define YM_METRO_MIN_BLOCKS 4   // resident 128-thread blocks per SM the register budget targets
+// Resident 128-thread blocks per SM the register budget targets: the staging
+// buffers (54 KB dynamic + the 18 KB accumulator per block) fit three blocks
+// per SM, and at three blocks 168 registers per thread leave no spills.
+#define YM_METRO_MIN_BLOCKS 3
 #endif
 
 namespace ym {
@@ -81,69 +85,116 @@ __device__ __forceinline__ m3 staged_link(const double2 (*buf)[T]) {
     return o;
 }
 
-// The two staple terms of direction NU for link (x, MU):
-//   forward  U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag
-//   backward U_nu(x-nu+mu)^dag U_mu(x-nu)^dag U_nu(x-nu)
-// P = first two factors (fma chains from zero), then A += P * third factor.
-template <int MU, int NU, bool RESIDENT = false>
-__device__ __forceinline__ void add_staple(const double2 *__restrict__ links, const ChainInfo &c,
-                                           const Coord &x, int par, const Nb &pm, double (*sa)[T],
-                                           double2 (*buf)[T]) {
-    const Nb pn = step(c, x.x, x.lex, par, NU, +1);
+// Staple sum A for link (x, MU): for each NU != MU in ascending order, the
+// forward term U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag, then the backward term
+// U_nu(x-nu+mu)^dag U_mu(x-nu)^dag U_nu(x-nu); P = the first two factors (fma
+// chains from zero), then A += P * third factor.  Every factor is staged by
+// cp.async: the first two one term ahead, the third at the start of its own
+// term, so each product starts on data that has already landed.
+struct TermSites {
+    int64_t s1, s2, s3;   // storage indices of the three factors
+};
+
+template <int MU, int NU, bool BWD>
+__device__ __forceinline__ TermSites term_sites(const ChainInfo &c, const Coord &x, int par,
+                                                const Nb &pm) {
+    if (!BWD) {
+        const Nb pn = step(c, x.x, x.lex, par, NU, +1);
+        return TermSites{storage_index(c, pm.lex, pm.par), storage_index(c, pn.lex, pn.par),
+                         storage_index(c, x.lex, par)};
+    }
     const Nb mn = step(c, x.x, x.lex, par, NU, -1);
-    const Nb mnpm = step(c, x.x, mn.lex, mn.par, MU, +1);   // x-nu keeps x's mu coordinate
+    const Nb mnpm = step(c, x.x, mn.lex, mn.par, MU, +1);
+    const int64_t smn = storage_index(c, mn.lex, mn.par);
+    return TermSites{storage_index(c, mnpm.lex, mnpm.par), smn, smn};
+}
+
+struct StageBufs {
+    double2 (*l1)[T];
+    double2 (*l2)[T];
+    double2 (*l3)[T];
+};
+
+__device__ __forceinline__ void stage_pair(const StageBufs &b, const double2 *links, const ChainInfo &c,
+                                           const TermSites &t, int d1, int d2) {
+    const double2 *p1 = links + c.offset + (int64_t)(d1 * 9) * c.volume + t.s1;
+    const double2 *p2 = links + c.offset + (int64_t)(d2 * 9) * c.volume + t.s2;
+#pragma unroll
+    for (int e = 0; e < 9; ++e) {
+        cp_async16(&b.l1[e][threadIdx.x], p1 + (int64_t)e * c.volume);
+        cp_async16(&b.l2[e][threadIdx.x], p2 + (int64_t)e * c.volume);
+    }
+    cp_async_commit();
+}
+
+__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+// Term (NU, BWD) with its sites `cur`; stages the next term's first two
+// factors (sites `nxt`, directions NNU / MU) when HAS_NEXT.
+template <int MU, int NU, bool BWD, bool HAS_NEXT, int NNU>
+__device__ __forceinline__ void staged_term(const double2 *links, const ChainInfo &c, const TermSites &cur,
+                                            const TermSites &nxt, const StageBufs &b, double (*sa)[T]) {
+    stage_link(b.l3, links, c, cur.s3, NU);
+    cp_async_wait_one();   // this term's first two factors have landed
+    m3 p;
     {
-        stage_link(buf, links, c, storage_index(c, x.lex, par), NU);
-        const m3 l2 = link_at<RESIDENT>(links, c, storage_index(c, pn.lex, pn.par), MU);
-        const m3 l1 = link_at<RESIDENT>(links, c, storage_index(c, pm.lex, pm.par), NU);
-        m3 p;
+        const m3 l1 = staged_link(b.l1), l2 = staged_link(b.l2);
 #pragma unroll
         for (int r = 0; r < 3; ++r)
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
                 cplx v = cmake(0.0, 0.0);
 #pragma unroll
-                for (int j = 0; j < 3; ++j) cfma(v, l1.e[r][j], cconj(l2.e[k][j]));
+                for (int j = 0; j < 3; ++j) {
+                    if (!BWD) cfma(v, l1.e[r][j], cconj(l2.e[k][j]));
+                    else cfma(v, cconj(l1.e[j][r]), cconj(l2.e[k][j]));
+                }
                 p.e[r][k] = v;
             }
-        cp_async_wait_all();
-        const m3 l3 = staged_link(buf);
-#pragma unroll
-        for (int r = 0; r < 3; ++r)
-#pragma unroll
-            for (int col = 0; col < 3; ++col) {
-                cplx a = sa_get(sa, 3 * r + col);
-#pragma unroll
-                for (int k = 0; k < 3; ++k) cfma(a, p.e[r][k], cconj(l3.e[col][k]));
-                sa_put(sa, 3 * r + col, a);
-            }
     }
-    {
-        stage_link(buf, links, c, storage_index(c, mn.lex, mn.par), NU);
-        const m3 l2 = link_at<RESIDENT>(links, c, storage_index(c, mn.lex, mn.par), MU);
-        const m3 l1 = link_at<RESIDENT>(links, c, storage_index(c, mnpm.lex, mnpm.par), NU);
-        m3 p;
+    if (HAS_NEXT) {
+        stage_pair(b, links, c, nxt, NNU, MU);
+        cp_async_wait_one();   // the third factor (older group) has landed
+    } else {
+        cp_async_wait_all();
+    }
+    const m3 l3 = staged_link(b.l3);
 #pragma unroll
-        for (int r = 0; r < 3; ++r)
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int col = 0; col < 3; ++col) {
+            cplx a = sa_get(sa, 3 * r + col);
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
-                cplx v = cmake(0.0, 0.0);
-#pragma unroll
-                for (int j = 0; j < 3; ++j) cfma(v, cconj(l1.e[j][r]), cconj(l2.e[k][j]));
-                p.e[r][k] = v;
+                if (!BWD) cfma(a, p.e[r][k], cconj(l3.e[col][k]));
+                else cfma(a, p.e[r][k], l3.e[k][col]);
             }
-        cp_async_wait_all();
-        const m3 l3 = staged_link(buf);
-#pragma unroll
-        for (int r = 0; r < 3; ++r)
-#pragma unroll
-            for (int col = 0; col < 3; ++col) {
-                cplx a = sa_get(sa, 3 * r + col);
-#pragma unroll
-                for (int k = 0; k < 3; ++k) cfma(a, p.e[r][k], l3.e[k][col]);
-                sa_put(sa, 3 * r + col, a);
-            }
-    }
+            sa_put(sa, 3 * r + col, a);
+        }
+}
+
+template <int MU, int I>
+struct Nu {   // the I-th direction other than MU
+    static constexpr int v = I < MU ? I : I + 1;
+};
+
+template <int MU>
+__device__ __forceinline__ void staple_pipelined(const double2 *links, const ChainInfo &c, const Coord &x,
+                                                 int par, const Nb &pm, double (*sa)[T], const StageBufs &b) {
+    constexpr int N0 = Nu<MU, 0>::v, N1 = Nu<MU, 1>::v, N2 = Nu<MU, 2>::v;
+    const TermSites t0 = term_sites<MU, N0, false>(c, x, par, pm);
+    const TermSites t1 = term_sites<MU, N0, true>(c, x, par, pm);
+    stage_pair(b, links, c, t0, N0, MU);
+    staged_term<MU, N0, false, true, N0>(links, c, t0, t1, b, sa);
+    const TermSites t2 = term_sites<MU, N1, false>(c, x, par, pm);
+    staged_term<MU, N0, true, true, N1>(links, c, t1, t2, b, sa);
+    const TermSites t3 = term_sites<MU, N1, true>(c, x, par, pm);
+    staged_term<MU, N1, false, true, N1>(links, c, t2, t3, b, sa);
+    const TermSites t4 = term_sites<MU, N2, false>(c, x, par, pm);
+    staged_term<MU, N1, true, true, N2>(links, c, t3, t4, b, sa);
+    const TermSites t5 = term_sites<MU, N2, true>(c, x, par, pm);
+    staged_term<MU, N2, false, true, N2>(links, c, t4, t5, b, sa);
+    staged_term<MU, N2, true, false, N2>(links, c, t5, t5, b, sa);
 }
 
 // Metropolis decision shared by the block and diagonal hits.
@@ -319,7 +370,10 @@ k_su3_metropolis(const ChainInfo *__restrict__ chains, const Tile *__restrict__ 
                  double2 *__restrict__ links, int parity, double angle, int uniform,
                  const uint64_t *__restrict__ sweep_ptr, unsigned long long *__restrict__ accepts) {
     __shared__ double sa[18][T];
-    __shared__ double2 l3buf[9][T];
+    extern __shared__ __align__(16) double2 stage_mem[];
+    const StageBufs bufs{reinterpret_cast<double2 (*)[T]>(stage_mem),
+                         reinterpret_cast<double2 (*)[T]>(stage_mem + 9 * T),
+                         reinterpret_cast<double2 (*)[T]>(stage_mem + 18 * T)};
     const Tile tile = tiles[blockIdx.x];
     const ChainInfo c = chains[tile.chain];
     const int64_t t = tile.start + threadIdx.x;
@@ -330,10 +384,7 @@ k_su3_metropolis(const ChainInfo *__restrict__ chains, const Tile *__restrict__ 
 #pragma unroll
         for (int e = 0; e < 18; ++e) sa[e][threadIdx.x] = 0.0;
         const Nb pm = step(c, x.x, x.lex, parity, MU, +1);
-        if (MU != 0) add_staple<MU, 0>(links, c, x, parity, pm, sa, l3buf);
-        if (MU != 1) add_staple<MU, 1>(links, c, x, parity, pm, sa, l3buf);
-        if (MU != 2) add_staple<MU, 2>(links, c, x, parity, pm, sa, l3buf);
-        if (MU != 3) add_staple<MU, 3>(links, c, x, parity, pm, sa, l3buf);
+        staple_pipelined<MU>(links, c, x, parity, pm, sa, bufs);
         m3 u = load_su3_rw(links, c, s, MU);
         const uint64_t key = link_key(c.seed, *sweep_ptr, x.lex, MU);
         accepted = visit(u, sa, c.beta / 3.0, angle, key, uniform);
@@ -357,14 +408,14 @@ k_su3_metropolis(const ChainInfo *__restrict__ chains, const Tile *__restrict__ 
 // ---- latency-oriented link update for the chain-resident kernel ----------
 // A resident launch has only a few hundred threads per sub-sweep, so the
 // time of a sub-sweep is the dependent-operation depth of one link update.
-// The functions below compute exactly the same values as add_staple/visit
+// The functions below compute exactly the same values as staple_pipelined/visit
 // with less depth: the staple sum stays in registers, the Taylor chains of
 // all eight hits (independent of the link) run in lockstep before the
 // first hit, the SU(2)-subgroup hits share one formula (so drawn
 // generators do not split a warp four ways), and most accept decisions come
 // from a bracket around exp(-m) instead of exp itself.
 
-// add_staple's two terms of direction NU, accumulated into a in registers
+// staple_pipelined's two terms of direction NU, accumulated into a in registers
 // (the same fma chains in the same order).
 template <int MU, int NU>
 __device__ __forceinline__ void add_staple_reg(const double2 *links, const ChainInfo &c,
@@ -661,13 +712,30 @@ __global__ void k_advance_sweep(uint64_t *sweep) { *sweep += 1; }
 
 }  // namespace
 
+constexpr size_t kStageBytes = 27 * T * sizeof(double2);   // three staged factors per thread
+
 cudaError_t launch_su3_metropolis(ym_ensemble *e, int parity, int mu, double angle, int uniform) {
+    static thread_local int configured_device = -1;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (configured_device != dev) {
+        const void *fns[4] = {(const void *)k_su3_metropolis<0>, (const void *)k_su3_metropolis<1>,
+                              (const void *)k_su3_metropolis<2>, (const void *)k_su3_metropolis<3>};
+        for (const void *f : fns) {
+            cudaError_t err = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageBytes);
+            if (err == cudaSuccess)
+                err = cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                           cudaSharedmemCarveoutMaxShared);
+            if (err != cudaSuccess) return err;
+        }
+        configured_device = dev;
+    }
     const dim3 grid((unsigned)e->n_half_tiles), block(T);
     switch (mu) {
-    case 0: k_su3_metropolis<0><<<grid, block, 0, e->stream>>>(e->d_chains, e->d_half_tiles, e->d_links, parity, angle, uniform, e->d_sweep, e->d_accepts); break;
-    case 1: k_su3_metropolis<1><<<grid, block, 0, e->stream>>>(e->d_chains, e->d_half_tiles, e->d_links, parity, angle, uniform, e->d_sweep, e->d_accepts); break;
-    case 2: k_su3_metropolis<2><<<grid, block, 0, e->stream>>>(e->d_chains, e->d_half_tiles, e->d_links, parity, angle, uniform, e->d_sweep, e->d_accepts); break;
-    default: k_su3_metropolis<3><<<grid, block, 0, e->stream>>>(e->d_chains, e->d_half_tiles, e->d_links, parity, angle, uniform, e->d_sweep, e->d_accepts); break;
+    case 0: k_su3_metropolis<0><<<grid, block, kStageBytes, e->stream>>>(e->d_chains, e->d_half_tiles, e->d_links, parity, angle, uniform, e->d_sweep, e->d_accepts); break;
+    case 1: k_su3_metropolis<1><<<grid, block, kStageBytes, e->stream>>>(e->d_chains, e->d_half_tiles, e->d_links, parity, angle, uniform, e->d_sweep, e->d_accepts); break;
+    case 2: k_su3_metropolis<2><<<grid, block, kStageBytes, e->stream>>>(e->d_chains, e->d_half_tiles, e->d_links, parity, angle, uniform, e->d_sweep, e->d_accepts); break;
+    default: k_su3_metropolis<3><<<grid, block, kStageBytes, e->stream>>>(e->d_chains, e->d_half_tiles, e->d_links, parity, angle, uniform, e->d_sweep, e->d_accepts); break;
     }
     return cudaGetLastError();
 }
