@@ -27,12 +27,14 @@ constexpr double kTermCutoff = 1.0e-18;           // EXP_TERM_CUTOFF su3.rs:25
 constexpr double kInvSqrt3 = 0.5773502691896258;  // su3.rs:22
 
 // c = 1 - t2 + t4 ..., s = t1 - t3 + ..., stopping after the first term with
-// |t_k| <= 1e-18, at most 64 terms (su3.rs:434-440).
+// |t_k| <= 1e-18, at most 64 terms (su3.rs:434-440).  Fully unrolled, so
+// every fl(1/k) is an immediate constant operand and the loop carries no
+// counter (about 2% of the FP64 sub-sweep).
 __device__ __forceinline__ void taylor_chain(double h, double &c, double &s) {
     double t = 1.0;
     c = 1.0;
     s = 0.0;
-#pragma unroll 1
+#pragma unroll
     for (int k = 1; k <= 64; k += 4) {
         t = (t * h) * c_inv[k];
         s = s + t;
@@ -55,7 +57,7 @@ __device__ __forceinline__ void taylor_chain2(double h1, double h2, double &c1, 
                                               double &c2, double &s2) {
     double t1 = 1.0, t2 = 1.0;
     c1 = 1.0; s1 = 0.0; c2 = 1.0; s2 = 0.0;
-#pragma unroll 1
+#pragma unroll
     for (int k = 1; k <= 64; k += 4) {
         t1 = (t1 * h1) * c_inv[k];     t2 = (t2 * h2) * c_inv[k];
         s1 = s1 + t1;                  s2 = s2 + t2;

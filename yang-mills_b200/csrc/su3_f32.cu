@@ -27,21 +27,28 @@ namespace {
 constexpr int T = kSweepThreads;
 using namespace f32;
 
+#ifndef YM_F32_MIN_BLOCKS
+#define YM_F32_MIN_BLOCKS 4
+#endif
+
 template <int MU>
-__global__ void __launch_bounds__(T)
+__global__ void __launch_bounds__(T, YM_F32_MIN_BLOCKS)
 k_f32_metropolis(const ChainInfo *__restrict__ chains, const Tile *__restrict__ tiles,
                  float2 *__restrict__ links, int parity, double angle, int uniform,
                  const uint64_t *__restrict__ sweep_ptr, unsigned long long *__restrict__ accepts) {
+    __shared__ __align__(16) float2 stage[18][T];   // 18 KB: three staged factors
+    const StageF<T> bufs{stage, stage + 6, stage + 12};
     const Tile tile = tiles[blockIdx.x];
     const ChainInfo c = chains[tile.chain];
     const int64_t t = tile.start + threadIdx.x;
+    const uint64_t sweep = *sweep_ptr;
     unsigned accepted = 0;
     if (t < c.half) {
         const int64_t s = (int64_t)parity * c.half + t;
         const Coord x = decode_storage(c, s);
-        const m3f a = staple_f<MU>(links, c, x, parity);
+        const m3f a = staple_f_staged<MU>(links, c, x, parity, bufs);
         m3f u = load_f(links, c, s, MU);
-        const uint64_t key = link_key(c.seed, *sweep_ptr, x.lex, MU);
+        const uint64_t key = link_key(c.seed, sweep, x.lex, MU);
         accepted = visit_f(u, a, c.beta / 3.0, angle, key, uniform);
         store_f(links, c, s, MU, u);
     }

@@ -153,6 +153,134 @@ __device__ __forceinline__ m3f staple_f(const float2 *__restrict__ links, const 
     return a;
 }
 
+// staple_f with every factor staged global -> shared by cp.async ahead of
+// its use: the first two factors of a term one term ahead, the third when
+// its own term starts, so each product starts on data that has landed and
+// loads in flight hold no registers.  Same terms, order and arithmetic as
+// staple_f, so the same bits.  Each thread owns column threadIdx.x of three
+// [6][TT] float2 buffers (two stored rows per link).
+template <int TT>
+struct StageF {
+    float2 (*l1)[TT];
+    float2 (*l2)[TT];
+    float2 (*l3)[TT];
+};
+
+template <int TT>
+__device__ __forceinline__ void stage_f(float2 (*buf)[TT], const float2 *links, const ChainInfo &c,
+                                        int64_t s, int mu) {
+    const float2 *p = links + c.offset + (int64_t)(mu * 6) * c.volume + s;
+#pragma unroll
+    for (int e = 0; e < 6; ++e) cp_async8(&buf[e][threadIdx.x], p + (int64_t)e * c.volume);
+}
+
+template <int TT>
+__device__ __forceinline__ m3f staged_f(const float2 (*buf)[TT]) {
+    m3f u;
+#pragma unroll
+    for (int e = 0; e < 6; ++e) {
+        const float2 v = buf[e][threadIdx.x];
+        u.e[e / 3][e % 3] = cfm(v.x, v.y);
+    }
+    third_row(u);
+    return u;
+}
+
+// Storage indices of a term's three factors.
+struct TermF {
+    int64_t s1, s2, s3;
+};
+
+template <int MU, int NU, bool BWD>
+__device__ __forceinline__ TermF term_f(const ChainInfo &c, const Coord &x, int par, const Nb &pm) {
+    if (!BWD) {
+        const Nb pn = step(c, x.x, x.lex, par, NU, +1);
+        return TermF{storage_index(c, pm.lex, pm.par), storage_index(c, pn.lex, pn.par),
+                     storage_index(c, x.lex, par)};
+    }
+    const Nb mn = step(c, x.x, x.lex, par, NU, -1);
+    const Nb mnpm = step(c, x.x, mn.lex, mn.par, MU, +1);
+    const int64_t smn = storage_index(c, mn.lex, mn.par);
+    return TermF{storage_index(c, mnpm.lex, mnpm.par), smn, smn};
+}
+
+// Term (NU, BWD) on sites `cur`; stages the next term's first two factors
+// (sites `nxt`, directions NNU / MU) when HAS_NEXT.
+template <int MU, int NU, bool BWD, bool HAS_NEXT, int NNU, int TT>
+__device__ __forceinline__ void staged_term_f(const float2 *links, const ChainInfo &c, const TermF &cur,
+                                              const TermF &nxt, const StageF<TT> &b, m3f &a) {
+    stage_f(b.l3, links, c, cur.s3, NU);
+    cp_async_commit();
+    cp_async_wait_one();   // this term's first two factors have landed
+    m3f p;
+    {
+        const m3f l1 = staged_f(b.l1), l2 = staged_f(b.l2);
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                cf v = cfm(0.f, 0.f);
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    if (!BWD) cffma(v, l1.e[r][j], cfconj(l2.e[k][j]));
+                    else cffma(v, cfconj(l1.e[j][r]), cfconj(l2.e[k][j]));
+                }
+                p.e[r][k] = v;
+            }
+    }
+    if (HAS_NEXT) {
+        stage_f(b.l1, links, c, nxt.s1, NNU);
+        stage_f(b.l2, links, c, nxt.s2, MU);
+        cp_async_commit();
+        cp_async_wait_one();   // the third factor (older group) has landed
+    } else {
+        cp_async_wait_all();
+    }
+    const m3f l3 = staged_f(b.l3);
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int col = 0; col < 3; ++col)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                if (!BWD) cffma(a.e[r][col], p.e[r][k], cfconj(l3.e[col][k]));
+                else cffma(a.e[r][col], p.e[r][k], l3.e[k][col]);
+            }
+}
+
+template <int MU, int I>
+struct NuF {   // the I-th direction other than MU
+    static constexpr int v = I < MU ? I : I + 1;
+};
+
+template <int MU, int TT>
+__device__ __forceinline__ m3f staple_f_staged(const float2 *links, const ChainInfo &c, const Coord &x,
+                                               int par, const StageF<TT> &b) {
+    constexpr int N0 = NuF<MU, 0>::v, N1 = NuF<MU, 1>::v, N2 = NuF<MU, 2>::v;
+    m3f a;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) a.e[i][j] = cfm(0.f, 0.f);
+    const Nb pm = step(c, x.x, x.lex, par, MU, +1);
+    const TermF t0 = term_f<MU, N0, false>(c, x, par, pm);
+    const TermF t1 = term_f<MU, N0, true>(c, x, par, pm);
+    stage_f(b.l1, links, c, t0.s1, N0);
+    stage_f(b.l2, links, c, t0.s2, MU);
+    cp_async_commit();
+    staged_term_f<MU, N0, false, true, N0>(links, c, t0, t1, b, a);
+    const TermF t2 = term_f<MU, N1, false>(c, x, par, pm);
+    staged_term_f<MU, N0, true, true, N1>(links, c, t1, t2, b, a);
+    const TermF t3 = term_f<MU, N1, true>(c, x, par, pm);
+    staged_term_f<MU, N1, false, true, N1>(links, c, t2, t3, b, a);
+    const TermF t4 = term_f<MU, N2, false>(c, x, par, pm);
+    staged_term_f<MU, N1, true, true, N2>(links, c, t3, t4, b, a);
+    const TermF t5 = term_f<MU, N2, true>(c, x, par, pm);
+    staged_term_f<MU, N2, false, true, N2>(links, c, t4, t5, b, a);
+    staged_term_f<MU, N2, true, false, N2>(links, c, t5, t5, b, a);
+    return a;
+}
+
 // Row i of Re Tr(X A) in binary64 from binary32 operands.
 __device__ __forceinline__ double retr_row64(const cf *xrow, const m3f &a, int i) {
     double acc = (double)xrow[0].re * (double)a.e[0][i].re;

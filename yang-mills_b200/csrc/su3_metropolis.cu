@@ -20,9 +20,9 @@
 // Layout: per thread the staple accumulator lives in shared memory (18
 // doubles per thread, conflict-free column layout), and every factor of the
 // six staple terms is copied global -> shared by cp.async ahead of its use
-// (the first two factors one term ahead, the third when its term starts), so
-// loads overlap the products without holding registers; three 128-thread
-// blocks fit per SM.
+// (the first two factors one term ahead, the third when its term starts, the
+// updated link itself during the last term), so loads overlap the products
+// without holding registers; three 128-thread blocks fit per SM.
 #include <cuda_runtime.h>
 
 #include "su3_exp.cuh"
@@ -55,16 +55,6 @@ __device__ __forceinline__ void sa_col(const double (*sa)[T], int i, cplx col[3]
 #pragma unroll
     for (int k = 0; k < 3; ++k) col[k] = sa_get(sa, 3 * k + i);
 }
-
-// Asynchronous 16-byte global -> shared copies (cp.async, L2 only): the
-// third factor of a staple term is fetched while the first product of the
-// term is computed, without holding registers for it.
-__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
-    const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 // Link (s, mu) into this thread's column of the staging buffer.
 __device__ __forceinline__ void stage_link(double2 (*buf)[T], const double2 *links, const ChainInfo &c,
@@ -127,10 +117,10 @@ __device__ __forceinline__ void stage_pair(const StageBufs &b, const double2 *li
     cp_async_commit();
 }
 
-__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
-
 // Term (NU, BWD) with its sites `cur`; stages the next term's first two
-// factors (sites `nxt`, directions NNU / MU) when HAS_NEXT.
+// factors (sites `nxt`, directions NNU / MU) when HAS_NEXT, else the updated
+// link U_MU at storage index nxt.s1 into the first buffer, so it lands
+// during the last product.
 template <int MU, int NU, bool BWD, bool HAS_NEXT, int NNU>
 __device__ __forceinline__ void staged_term(const double2 *links, const ChainInfo &c, const TermSites &cur,
                                             const TermSites &nxt, const StageBufs &b, double (*sa)[T]) {
@@ -156,7 +146,8 @@ __device__ __forceinline__ void staged_term(const double2 *links, const ChainInf
         stage_pair(b, links, c, nxt, NNU, MU);
         cp_async_wait_one();   // the third factor (older group) has landed
     } else {
-        cp_async_wait_all();
+        stage_link(b.l1, links, c, nxt.s1, MU);   // the updated link itself (sites `nxt`)
+        cp_async_wait_one();
     }
     const m3 l3 = staged_link(b.l3);
 #pragma unroll
@@ -180,7 +171,8 @@ struct Nu {   // the I-th direction other than MU
 
 template <int MU>
 __device__ __forceinline__ void staple_pipelined(const double2 *links, const ChainInfo &c, const Coord &x,
-                                                 int par, const Nb &pm, double (*sa)[T], const StageBufs &b) {
+                                                 int par, const Nb &pm, double (*sa)[T], const StageBufs &b,
+                                                 int64_t s_self) {
     constexpr int N0 = Nu<MU, 0>::v, N1 = Nu<MU, 1>::v, N2 = Nu<MU, 2>::v;
     const TermSites t0 = term_sites<MU, N0, false>(c, x, par, pm);
     const TermSites t1 = term_sites<MU, N0, true>(c, x, par, pm);
@@ -194,7 +186,7 @@ __device__ __forceinline__ void staple_pipelined(const double2 *links, const Cha
     staged_term<MU, N1, true, true, N2>(links, c, t3, t4, b, sa);
     const TermSites t5 = term_sites<MU, N2, true>(c, x, par, pm);
     staged_term<MU, N2, false, true, N2>(links, c, t4, t5, b, sa);
-    staged_term<MU, N2, true, false, N2>(links, c, t5, t5, b, sa);
+    staged_term<MU, N2, true, false, N2>(links, c, t5, TermSites{s_self, 0, 0}, b, sa);
 }
 
 // Metropolis decision shared by the block and diagonal hits.
@@ -377,6 +369,7 @@ k_su3_metropolis(const ChainInfo *__restrict__ chains, const Tile *__restrict__ 
     const Tile tile = tiles[blockIdx.x];
     const ChainInfo c = chains[tile.chain];
     const int64_t t = tile.start + threadIdx.x;
+    const uint64_t sweep = *sweep_ptr;
     unsigned accepted = 0;
     if (t < c.half) {
         const int64_t s = (int64_t)parity * c.half + t;
@@ -384,9 +377,10 @@ k_su3_metropolis(const ChainInfo *__restrict__ chains, const Tile *__restrict__ 
 #pragma unroll
         for (int e = 0; e < 18; ++e) sa[e][threadIdx.x] = 0.0;
         const Nb pm = step(c, x.x, x.lex, parity, MU, +1);
-        staple_pipelined<MU>(links, c, x, parity, pm, sa, bufs);
-        m3 u = load_su3_rw(links, c, s, MU);
-        const uint64_t key = link_key(c.seed, *sweep_ptr, x.lex, MU);
+        staple_pipelined<MU>(links, c, x, parity, pm, sa, bufs, s);
+        cp_async_wait_all();
+        m3 u = staged_link(bufs.l1);
+        const uint64_t key = link_key(c.seed, sweep, x.lex, MU);
         accepted = visit(u, sa, c.beta / 3.0, angle, key, uniform);
         store_su3(links, c, s, MU, u);
     }

@@ -203,6 +203,23 @@ __device__ __forceinline__ double grid_angle(uint64_t raw, double angle) {
     return sign * magnitude;
 }
 
+// ------------------------------------------------- asynchronous staging
+// Global -> shared copies (cp.async) that land while the thread computes,
+// without holding registers for the data: 16 bytes through L2 only, 8 bytes
+// through L1 (the 8-byte form has no L2-only variant).  Groups are
+// committed per batch and waited for oldest first.
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
+    const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
 // ---------------------------------------------------------------- geometry
 
 // One chain of an ensemble.  Sites are stored in checkerboard order when the
@@ -245,12 +262,25 @@ __device__ __forceinline__ Coord decode_storage(const ChainInfo &c, int64_t s) {
         int par = s >= c.half ? 1 : 0;
         int64_t t = s - (int64_t)par * c.half;
         int64_t two_t = 2 * t;
-        int64_t row = two_t / c.n[3];
-        int x3b = (int)(two_t - row * c.n[3]);
-        k.x[2] = (int)(row % c.n[2]);
-        int64_t r2 = row / c.n[2];
-        k.x[1] = (int)(r2 % c.n[1]);
-        k.x[0] = (int)(r2 / c.n[1]);
+        int x3b;
+        if (c.volume <= 0x7fffffff) {
+            // 32-bit divisions (a few instructions each instead of a 64-bit
+            // division routine) whenever every site index fits.
+            const uint32_t tt = (uint32_t)two_t, n3 = (uint32_t)c.n[3];
+            const uint32_t n2 = (uint32_t)c.n[2], n1 = (uint32_t)c.n[1];
+            const uint32_t r1 = tt / n3, r2 = r1 / n2, r3 = r2 / n1;
+            x3b = (int)(tt - r1 * n3);
+            k.x[2] = (int)(r1 - r2 * n2);
+            k.x[1] = (int)(r2 - r3 * n1);
+            k.x[0] = (int)r3;
+        } else {
+            int64_t row = two_t / c.n[3];
+            x3b = (int)(two_t - row * c.n[3]);
+            k.x[2] = (int)(row % c.n[2]);
+            int64_t r2 = row / c.n[2];
+            k.x[1] = (int)(r2 % c.n[1]);
+            k.x[0] = (int)(r2 / c.n[1]);
+        }
         int b = (par + k.x[0] + k.x[1] + k.x[2]) & 1;
         k.x[3] = x3b + b;
         lex = two_t + b;
