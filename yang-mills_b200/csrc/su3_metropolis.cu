@@ -17,8 +17,8 @@
 //     written as fixed chains of fma() that the CPU oracle repeats bit for
 //     bit.
 //
-// Layout: per thread the staple accumulator lives in shared memory (18
-// doubles per thread, conflict-free column layout), and every factor of the
+// Layout: per thread the staple accumulator lives in shared memory (nine
+// double2 per thread, conflict-free column layout), and every factor of the
 // six staple terms is copied global -> shared by cp.async ahead of its use
 // (the first two factors one term ahead, the third when its term starts, the
 // updated link itself during the last term), so loads overlap the products
@@ -42,16 +42,16 @@ namespace {
 
 constexpr int T = kSweepThreads;
 
-__device__ __forceinline__ cplx sa_get(const double (*sa)[T], int e) {
-    return cmake(sa[2 * e][threadIdx.x], sa[2 * e + 1][threadIdx.x]);
+__device__ __forceinline__ cplx sa_get(const double2 (*sa)[T], int e) {
+    const double2 v = sa[e][threadIdx.x];
+    return cmake(v.x, v.y);
 }
-__device__ __forceinline__ void sa_put(double (*sa)[T], int e, cplx v) {
-    sa[2 * e][threadIdx.x] = v.re;
-    sa[2 * e + 1][threadIdx.x] = v.im;
+__device__ __forceinline__ void sa_put(double2 (*sa)[T], int e, cplx v) {
+    sa[e][threadIdx.x] = make_double2(v.re, v.im);
 }
 
 // Column i of A: A[0][i], A[1][i], A[2][i].
-__device__ __forceinline__ void sa_col(const double (*sa)[T], int i, cplx col[3]) {
+__device__ __forceinline__ void sa_col(const double2 (*sa)[T], int i, cplx col[3]) {
 #pragma unroll
     for (int k = 0; k < 3; ++k) col[k] = sa_get(sa, 3 * k + i);
 }
@@ -123,7 +123,7 @@ __device__ __forceinline__ void stage_pair(const StageBufs &b, const double2 *li
 // during the last product.
 template <int MU, int NU, bool BWD, bool HAS_NEXT, int NNU>
 __device__ __forceinline__ void staged_term(const double2 *links, const ChainInfo &c, const TermSites &cur,
-                                            const TermSites &nxt, const StageBufs &b, double (*sa)[T]) {
+                                            const TermSites &nxt, const StageBufs &b, double2 (*sa)[T]) {
     stage_link(b.l3, links, c, cur.s3, NU);
     cp_async_wait_one();   // this term's first two factors have landed
     m3 p;
@@ -171,7 +171,7 @@ struct Nu {   // the I-th direction other than MU
 
 template <int MU>
 __device__ __forceinline__ void staple_pipelined(const double2 *links, const ChainInfo &c, const Coord &x,
-                                                 int par, const Nb &pm, double (*sa)[T], const StageBufs &b,
+                                                 int par, const Nb &pm, double2 (*sa)[T], const StageBufs &b,
                                                  int64_t s_self) {
     constexpr int N0 = Nu<MU, 0>::v, N1 = Nu<MU, 1>::v, N2 = Nu<MU, 2>::v;
     const TermSites t0 = term_sites<MU, N0, false>(c, x, par, pm);
@@ -201,7 +201,7 @@ __device__ __forceinline__ bool accept_step(double old_tr, double new_tr, double
 // [[c, s],[-s, c]] (kind 1) or diag(c + i s, c - i s) (kind 2).  Candidate
 // rows are Mat3::mul's values (no fused multiply-add).
 template <int I0, int I1>
-__device__ __forceinline__ void hit_block(m3 &u, const double (*sa)[T], double rr[3], double &old_tr,
+__device__ __forceinline__ void hit_block(m3 &u, const double2 (*sa)[T], double rr[3], double &old_tr,
                                           int kind, double c, double s, double beta3, double unif,
                                           unsigned &accepted) {
     cplx n0[3], n1[3];
@@ -240,7 +240,7 @@ __device__ __forceinline__ void hit_block(m3 &u, const double (*sa)[T], double r
     }
 }
 
-__device__ __forceinline__ void hit_diag(m3 &u, const double (*sa)[T], double rr[3], double &old_tr,
+__device__ __forceinline__ void hit_diag(m3 &u, const double2 (*sa)[T], double rr[3], double &old_tr,
                                          cplx e1, cplx e2, double beta3, double unif,
                                          unsigned &accepted) {
     cplx n[3][3];
@@ -273,7 +273,7 @@ __device__ __forceinline__ void hit_diag(m3 &u, const double (*sa)[T], double rr
 // hit_block writes its candidate entries as c*x + s*a with a one of the
 // other entries or its negation (c*x - s*y == c*x + s*(-y) exactly), so the
 // single formula gives hit_block's bits.
-__device__ __forceinline__ void hit_block_drawn(m3 &u, const double (*sa)[T], double rr[3],
+__device__ __forceinline__ void hit_block_drawn(m3 &u, const double2 (*sa)[T], double rr[3],
                                                 double &old_tr, int g, double c, double s,
                                                 double beta3, double unif, unsigned &accepted) {
     const int kind = (g == 2) ? 2 : ((g == 1 || g == 4 || g == 6) ? 1 : 0);
@@ -315,7 +315,7 @@ __device__ __forceinline__ void hit_block_drawn(m3 &u, const double (*sa)[T], do
 
 // Eight hits on u: generator h (ordered) or bits 52..54 of the hit's angle
 // word (uniform).  Words 2h and 2h+1 of the link's stream.
-__device__ __forceinline__ unsigned visit(m3 &u, const double (*sa)[T], double beta3,
+__device__ __forceinline__ unsigned visit(m3 &u, const double2 (*sa)[T], double beta3,
                                           double angle, uint64_t key, int uniform) {
     double rr[3];
 #pragma unroll
@@ -361,7 +361,7 @@ __global__ void __launch_bounds__(T, YM_METRO_MIN_BLOCKS)
 k_su3_metropolis(const ChainInfo *__restrict__ chains, const Tile *__restrict__ tiles,
                  double2 *__restrict__ links, int parity, double angle, int uniform,
                  const uint64_t *__restrict__ sweep_ptr, unsigned long long *__restrict__ accepts) {
-    __shared__ double sa[18][T];
+    __shared__ double2 sa[9][T];
     extern __shared__ __align__(16) double2 stage_mem[];
     const StageBufs bufs{reinterpret_cast<double2 (*)[T]>(stage_mem),
                          reinterpret_cast<double2 (*)[T]>(stage_mem + 9 * T),
@@ -375,7 +375,7 @@ k_su3_metropolis(const ChainInfo *__restrict__ chains, const Tile *__restrict__ 
         const int64_t s = (int64_t)parity * c.half + t;
         const Coord x = decode_storage(c, s);
 #pragma unroll
-        for (int e = 0; e < 18; ++e) sa[e][threadIdx.x] = 0.0;
+        for (int e = 0; e < 9; ++e) sa[e][threadIdx.x] = make_double2(0.0, 0.0);
         const Nb pm = step(c, x.x, x.lex, parity, MU, +1);
         staple_pipelined<MU>(links, c, x, parity, pm, sa, bufs, s);
         cp_async_wait_all();
