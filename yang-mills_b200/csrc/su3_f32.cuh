@@ -386,9 +386,11 @@ __device__ __forceinline__ void hit_any_f(m3f &u, const m3f &a, double rr[3], do
                                           float theta, double beta3, double unif,
                                           unsigned &accepted) {
     const bool diag = g == 7;
-    float s1, c1, s2, c2;
+    float s1, c1;
     sincosf(diag ? theta * 0.28867513459481287f : 0.5f * theta, &s1, &c1);
-    sincosf(theta * -0.57735026918962573f, &s2, &c2);
+    // e^{-2 i phi} of lambda_8 from the same pair by the double-angle
+    // identities (one sincosf per hit instead of two)
+    const float c2 = fmaf(c1, c1, -s1 * s1), s2 = -2.f * s1 * c1;
     const int kind = diag ? 3 : ((g == 2) ? 2 : ((g == 1 || g == 4 || g == 6) ? 1 : 0));
     const cf zero = cfm(0.f, 0.f);
     const cf r00 = (kind == 0 || kind == 1) ? cfm(c1, 0.f) : cfm(c1, s1);
