@@ -361,6 +361,31 @@ def main():
                           "kernel": "k_stout_level (staples, Q, Cayley-Hamilton exponential "
                                     "with the reference's checks, per spatial link)"}}
 
+    # observables of the thermalised 32^4 FP64 lattice, each call timed by the
+    # handle's CUDA-event pair around its kernels: Wilson loops R x T <= 4 x 4
+    # in all six planes, the Polyakov loop along direction 3, the A1++
+    # operator basis (spatial plaquettes and 2x1 rectangles per timeslice).
+    # Compulsory traffic: each link the observable reads, once (4V links for
+    # the loops, V for the Polyakov loop, 3V spatial links for the operators).
+    def obs_leg(kernel, call, n_links, reps=3):
+        call()
+        ens.profile(True)
+        for _ in range(reps):
+            call()
+        o_ms, o_n = ens.profile_read(kernel)
+        ens.profile(False)
+        o_s = o_ms * 1e-3 / max(1, o_n)
+        o_bytes = volume * n_links * LINK_BYTES
+        return {"ms": o_s * 1e3, "calls_timed": o_n, "compulsory_bytes": o_bytes,
+                "achieved_gbs": o_bytes / o_s / 1e9, "frac": o_bytes / o_s / 1e9 / peak}
+
+    observables = {
+        "wilson_loops_4x4_all_planes": obs_leg("aux", lambda: ens.wilson_loops(4, 4), 4),
+        "polyakov_loop_dir3": obs_leg("aux", lambda: ens.polyakov_loops(3), 1),
+        "a1pp_operator_basis": obs_leg("operators", ens.scalar_operator_basis, 3),
+        "peak_gbs": peak, "peak_source": f"{peak_kind} hbm_gbs",
+        "note": "per call on the 32^4 FP64 lattice; achieved = compulsory bytes / CUDA-event time"}
+
     # plaquette ESS/s of the three samplers at 16 x 16^4 from one equilibrated state
     def ess_leg(e, run):
         e.synchronize()
@@ -412,12 +437,23 @@ def main():
             e2.markov_sweeps(1, 3, sampler="kennedy-pendleton")
             series[i] = e2.average_plaquette()[0]
         secs = time.perf_counter() - t
+        # per-launch device time of the two update kernels (one launch = one
+        # parity and direction: 5,000 links), 20 more sweeps under the events
+        e2.profile(True)
+        e2.markov_sweeps(20, 3, sampler="kennedy-pendleton")
+        hb_ms, hb_n = e2.profile_read("su2_heatbath")
+        or_ms, or_n = e2.profile_read("su2_overrelax")
+        e2.profile(False)
         e2.close()
         d2 = diagnostics(series, 100)[0]
         out["su2_10^4_beta2.3_kp+3or"] = {
             "link_steps_per_s": world * 40000 * 4 * 500 / secs, "ms_per_sweep": 1e3 * secs / 500,
             "plaquette_mean": float(series.mean()), "plaquette_ess_per_s": world * d2.effective_sample_size / secs,
-            "note": "200 + 500 sweeps from a cold start, plaquette every sweep (read back each sweep)"}
+            "heatbath_us_per_launch": 1e3 * hb_ms / max(1, hb_n),
+            "overrelax_us_per_launch": 1e3 * or_ms / max(1, or_n),
+            "note": "200 + 500 sweeps from a cold start, plaquette every sweep (read back each sweep); "
+                    "per-launch times from 20 further sweeps under CUDA events (1.28 MB lattice, "
+                    "L2-resident: absolute rates, not an HBM fraction)"}
         # SU(3) 64 x 4^4 beta=6.0 FP64, generator uniform in 1..8, half width 0.3
         seeds = [derive_su3_chain_seed(MASTER_SEED, rank * 64 + i) for i in range(64)]
         e1 = ymgpu.Ensemble([[4, 4, 4, 4]] * 64, BETA, seeds, device=local)
@@ -554,6 +590,7 @@ def main():
                              "mean_generator_probabilities": [float(v) for v in p_gen.mean(0)]}},
             "other_configs": configs_extra,
             "stout_32x4_fp64": stout,
+            "observables_32x4_fp64": observables,
             "ess": {
                 "geometry": f"{ESS_CHAINS} chains x 16^4 (total volume of 32^4), beta=6.0, "
                             f"{n} measured sweeps per sampler from one equilibrated state",

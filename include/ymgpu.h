@@ -306,7 +306,8 @@ int32_t ym_sampling_efficiency(const double *values, int64_t n, const double *lo
  * proposals only) ----  While enabled, each launch of the listed kernels is
  * bracketed by CUDA events on the handle's stream; ym_profile_read
  * synchronises, returns the summed device time and launch count of one
- * kernel since the last read, and resets it. */
+ * kernel since the last read, and resets it.  YM_KERNEL_AUX covers the
+ * Wilson-loop and Polyakov-loop measurements (one bracket per call). */
 enum { YM_KERNEL_SU3_METROPOLIS = 0, YM_KERNEL_PLAQUETTE = 1, YM_KERNEL_SU2_HEATBATH = 2,
        YM_KERNEL_SU2_OVERRELAX = 3, YM_KERNEL_STOUT = 4, YM_KERNEL_OPERATORS = 5,
        YM_KERNEL_AUX = 6, YM_KERNEL_LEARNED = 7, YM_KERNEL_COUNT = 8 };

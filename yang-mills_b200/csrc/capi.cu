@@ -777,7 +777,7 @@ int32_t ym_su3_polyakov_loops(ym_ensemble *e, int32_t direction, double *out) {
     int32_t st = set_device(e);
     if (st) return st;
     YM_CUDA(ensure_obs_scratch(e));
-    YM_CUDA(ym::launch_polyakov(e, direction, e->d_obs_partial, e->d_obs_out));
+    YM_CUDA(timed(e, YM_KERNEL_AUX, [&] { return ym::launch_polyakov(e, direction, e->d_obs_partial, e->d_obs_out); }));
     YM_CUDA(cudaMemcpyAsync(out, e->d_obs_out, (size_t)e->n_chains * 2 * sizeof(double),
                             cudaMemcpyDeviceToHost, e->stream));
     YM_CUDA(cudaStreamSynchronize(e->stream));
