@@ -1,7 +1,9 @@
 """Gauge observables and glueball transformations on the B200 vs the oracle.
 
-Bars: per-site holonomies are computed in the reference's product order, so
-lattice means agree with the oracle's sequential sums to <= 1e-12 relative;
+Bars: per-site holonomies are evaluated as Re Tr of their two half-paths
+(each in traversal order) and Polyakov lines as ordered products, so lattice
+means agree with the oracle's single-chain, sequential-sum values to
+<= 1e-12 relative;
 stout smearing and blocking reproduce the reference goldens to 1e-12 and the
 oracle's smeared links to 1e-14.
 """
