@@ -95,7 +95,8 @@ __device__ __forceinline__ q4 link_q(const double2 *links, const ChainInfo &c, c
 }
 
 // Lattice4::staple (lib.rs:507-546): the unnormalised sum of six products,
-// nu ascending, forward then backward, components added in order.
+// nu ascending, forward then backward, components added in order (one
+// thread per link).
 template <int MU>
 __device__ __forceinline__ void su2_staple(const double2 *__restrict__ links, const ChainInfo &c,
                                            const Coord &x, int par, double comp[4]) {
@@ -117,6 +118,73 @@ __device__ __forceinline__ void su2_staple(const double2 *__restrict__ links, co
 #pragma unroll
         for (int i = 0; i < 4; ++i) comp[i] += bwd.c[i];
     }
+}
+
+// The same staple for a link updated by a group of kGroup lanes: lane j < 6
+// computes term j (the (j/2)-th direction nu != MU, forward for even j,
+// backward for odd j) and every lane of the group then adds the six terms in
+// that order, so the sum has the one-thread staple's bits while its twelve
+// normalised products run on six lanes at once.
+constexpr int kGroup = 8;
+constexpr int kGroupLinks = T / kGroup;   // links per 128-thread block
+
+__device__ __forceinline__ q4 qdag_if(const q4 &a, bool d) {
+    const double s = d ? -1.0 : 1.0;   // exact sign flip
+    return q4{{a.c[0], s * a.c[1], s * a.c[2], s * a.c[3]}};
+}
+
+__device__ __forceinline__ int32_t coord_of(const int32_t *x, int d) {
+    return d == 0 ? x[0] : (d == 1 ? x[1] : (d == 2 ? x[2] : x[3]));
+}
+
+// Neighbour along a direction chosen per lane (selects, no indexed arrays).
+__device__ __forceinline__ Nb step_any(const ChainInfo &c, const int32_t *x, int64_t lex, int par,
+                                       int d, int dir) {
+    const int32_t xd = coord_of(x, d), nd = coord_of(c.n, d);
+    const int64_t st = d == 3 ? 1 : (d == 2 ? (int64_t)c.n[3]
+                                            : (d == 1 ? (int64_t)c.n[2] * c.n[3]
+                                                      : (int64_t)c.n[1] * c.n[2] * c.n[3]));
+    const bool wrap = dir > 0 ? (xd == nd - 1) : (xd == 0);
+    const int64_t nl = dir > 0 ? (wrap ? lex - (int64_t)(nd - 1) * st : lex + st)
+                               : (wrap ? lex + (int64_t)(nd - 1) * st : lex - st);
+    const int flip = (wrap && (nd & 1)) ? 0 : 1;
+    return Nb{nl, par ^ flip};
+}
+
+// Term j of the staple of link (x, MU):
+//   forward  U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag
+//   backward U_nu(x-nu+mu)^dag U_mu(x-nu)^dag U_nu(x-nu)
+template <int MU>
+__device__ __forceinline__ q4 su2_staple_term(const double2 *__restrict__ links, const ChainInfo &c,
+                                              const Coord &x, int par, int j) {
+    const int k = j >> 1;
+    const int nu = k < MU ? k : k + 1;
+    const bool fwd = (j & 1) == 0;
+    const Nb pm = step(c, x.x, x.lex, par, MU, +1);
+    const Nb pn = step_any(c, x.x, x.lex, par, nu, +1);
+    const Nb mn = step_any(c, x.x, x.lex, par, nu, -1);
+    const Nb mnpm = step(c, x.x, mn.lex, mn.par, MU, +1);   // x - nu keeps x's mu coordinate
+    const Nb sa = fwd ? pm : mnpm, sb = fwd ? pn : mn, sc = fwd ? Nb{x.lex, par} : mn;
+    const q4 a = qdag_if(link_q(links, c, sa, nu), !fwd);
+    const q4 b = qdag(link_q(links, c, sb, MU));
+    const q4 cc = qdag_if(link_q(links, c, sc, nu), fwd);
+    return qmul(qmul(a, b), cc);
+}
+
+// The group's staple sum (every lane of the group gets it): terms computed
+// by lanes 0..5 of the group (`active` false: the group's lanes load nothing
+// and the sum is meaningless), added in term order.
+template <int MU>
+__device__ __forceinline__ void su2_staple_group(const double2 *__restrict__ links, const ChainInfo &c,
+                                                 const Coord &x, int par, bool active, double comp[4]) {
+    const int lane = threadIdx.x & 31, j = lane & (kGroup - 1), base = lane - j;
+    q4 term{{0.0, 0.0, 0.0, 0.0}};
+    if (active && j < 6) term = su2_staple_term<MU>(links, c, x, par, j);
+    comp[0] = comp[1] = comp[2] = comp[3] = 0.0;
+#pragma unroll
+    for (int jj = 0; jj < 6; ++jj)
+#pragma unroll
+        for (int i = 0; i < 4; ++i) comp[i] += __shfl_sync(0xffffffffu, term.c[i], base + jj);
 }
 
 // staple_norm (su2_ensemble.rs:194-202): sum of squares from -0.0, sqrt.
@@ -195,9 +263,10 @@ __device__ __forceinline__ bool sample_kp(double alpha, uint64_t key, int max_at
 constexpr unsigned kErrAttempts = 1u;
 constexpr unsigned kErrNonFinite = 2u;
 
+// One thread per link (large sub-sweeps, throughput-bound).
 template <int MU>
 __global__ void __launch_bounds__(T)
-k_su2_heatbath(const ChainInfo *__restrict__ chains, const Tile *__restrict__ tiles,
+k_su2_heatbath_thread(const ChainInfo *__restrict__ chains, const Tile *__restrict__ tiles,
                double2 *__restrict__ links, int parity, int max_attempts, int kp,
                const uint64_t *__restrict__ sweep_ptr, unsigned long long *__restrict__ proposals,
                unsigned *__restrict__ err) {
@@ -241,7 +310,7 @@ k_su2_heatbath(const ChainInfo *__restrict__ chains, const Tile *__restrict__ ti
 
 template <int MU>
 __global__ void __launch_bounds__(T)
-k_su2_overrelax(const ChainInfo *__restrict__ chains, const Tile *__restrict__ tiles,
+k_su2_overrelax_thread(const ChainInfo *__restrict__ chains, const Tile *__restrict__ tiles,
                 double2 *__restrict__ links, int parity, unsigned *__restrict__ err) {
     const Tile tile = tiles[blockIdx.x];
     const ChainInfo c = chains[tile.chain];
@@ -261,6 +330,84 @@ k_su2_overrelax(const ChainInfo *__restrict__ chains, const Tile *__restrict__ t
     normalize_scaled<4>(comp, vhat.c);
     const q4 nd = qdag(vhat);
     store_q(links, c, s, MU, qmul(qmul(nd, qdag(load_q_rw(links, c, s, MU))), nd));
+}
+
+// Grouped form (small sub-sweeps, latency-bound: a 10^4 lattice updates
+// 5,000 links per launch, about one warp per SM with one thread per link).
+// One block: kGroupLinks links of the tile blockIdx.x / kGroup (sub-block
+// blockIdx.x % kGroup), kGroup lanes per link; the update is evaluated by
+// every lane of the group alike and written by its first lane.
+template <int MU>
+__global__ void __launch_bounds__(T)
+k_su2_heatbath_group(const ChainInfo *__restrict__ chains, const Tile *__restrict__ tiles,
+               double2 *__restrict__ links, int parity, int max_attempts, int kp,
+               const uint64_t *__restrict__ sweep_ptr, unsigned long long *__restrict__ proposals,
+               unsigned *__restrict__ err) {
+    const Tile tile = tiles[blockIdx.x / kGroup];
+    const ChainInfo c = chains[tile.chain];
+    const int64_t t = tile.start + (int64_t)(blockIdx.x % kGroup) * kGroupLinks + threadIdx.x / kGroup;
+    const bool leader = (threadIdx.x & (kGroup - 1)) == 0;
+    const bool active = t < c.half;
+    const int64_t s = (int64_t)parity * c.half + (active ? t : 0);
+    const Coord x = decode_storage(c, s);
+    double comp[4];
+    su2_staple_group<MU>(links, c, x, parity, active, comp);
+    unsigned attempts_used = 0;
+    if (active) {
+        const double norm = staple_norm(comp);
+        const double alpha = c.beta * norm;
+        if (!isfinite(norm) || !isfinite(alpha)) {
+            if (leader) atomicOr(err, kErrNonFinite);
+        } else {
+            const uint64_t key = link_key(c.seed, *sweep_ptr, x.lex, MU);
+            q4 r;
+            int att = 0;
+            const bool ok = kp ? sample_kp(alpha, key, max_attempts, r, att)
+                               : sample_reference(alpha, key, max_attempts, r, att);
+            attempts_used = leader ? (unsigned)att : 0u;
+            if (!ok) {
+                if (leader) atomicOr(err, kErrAttempts);
+            } else {
+                q4 next = r;
+                if (norm != 0.0) {
+                    q4 vhat;
+                    normalize_scaled<4>(comp, vhat.c);
+                    next = qmul(r, qdag(vhat));
+                }
+                if (leader) store_q(links, c, s, MU, next);
+            }
+        }
+    }
+    const unsigned warp_sum = __reduce_add_sync(0xffffffffu, attempts_used);
+    if ((threadIdx.x & 31) == 0 && warp_sum)
+        atomicAdd(proposals + tile.chain, (unsigned long long)warp_sum);
+}
+
+template <int MU>
+__global__ void __launch_bounds__(T)
+k_su2_overrelax_group(const ChainInfo *__restrict__ chains, const Tile *__restrict__ tiles,
+                double2 *__restrict__ links, int parity, unsigned *__restrict__ err) {
+    const Tile tile = tiles[blockIdx.x / kGroup];
+    const ChainInfo c = chains[tile.chain];
+    const int64_t t = tile.start + (int64_t)(blockIdx.x % kGroup) * kGroupLinks + threadIdx.x / kGroup;
+    const bool leader = (threadIdx.x & (kGroup - 1)) == 0;
+    const bool active = t < c.half;
+    const int64_t s = (int64_t)parity * c.half + (active ? t : 0);
+    const Coord x = decode_storage(c, s);
+    double comp[4];
+    su2_staple_group<MU>(links, c, x, parity, active, comp);
+    if (!active) return;
+    const double norm = staple_norm(comp);
+    if (!isfinite(norm)) {
+        if (leader) atomicOr(err, kErrNonFinite);
+        return;
+    }
+    if (norm == 0.0) return;
+    q4 vhat;
+    normalize_scaled<4>(comp, vhat.c);
+    const q4 nd = qdag(vhat);
+    const q4 next = qmul(qmul(nd, qdag(load_q_rw(links, c, s, MU))), nd);
+    if (leader) store_q(links, c, s, MU, next);
 }
 
 // Plaquette half real trace per site, (mu, nu) order as the reference.
@@ -381,28 +528,67 @@ int grid_for(int64_t n, int threads) {
 
 }  // namespace
 
+// The grouped kernels give each link kGroup lanes; they win while a
+// sub-sweep has too few links to hide the one-thread kernels' latency
+// (measured on B200: 5,000 links per launch 15.5 vs 24.5 us heat-bath,
+// 32,768 links 35.4 vs 25.2 us, crossover near 17,000), so up to 96 links
+// per SM.
+static bool su2_grouped(const ym_ensemble *e) {
+    static thread_local int sms = 0, dev_seen = -1;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev != dev_seen) {
+        sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        dev_seen = dev;
+    }
+    return e->n_half_tiles * (int64_t)T <= (int64_t)sms * 96;
+}
+
 cudaError_t launch_su2_heatbath(ym_ensemble *e, int parity, int mu, int max_attempts, int kp) {
-    const dim3 g((unsigned)e->n_half_tiles), b(T);
     auto *ch = e->d_chains;
     auto *tl = e->d_half_tiles;
+    const dim3 b(T);
+    if (su2_grouped(e)) {
+        const dim3 g((unsigned)(e->n_half_tiles * kGroup));
+        switch (mu) {
+        case 0: k_su2_heatbath_group<0><<<g, b, 0, e->stream>>>(ch, tl, e->d_links, parity, max_attempts, kp, e->d_sweep, e->d_accepts, e->d_error); break;
+        case 1: k_su2_heatbath_group<1><<<g, b, 0, e->stream>>>(ch, tl, e->d_links, parity, max_attempts, kp, e->d_sweep, e->d_accepts, e->d_error); break;
+        case 2: k_su2_heatbath_group<2><<<g, b, 0, e->stream>>>(ch, tl, e->d_links, parity, max_attempts, kp, e->d_sweep, e->d_accepts, e->d_error); break;
+        default: k_su2_heatbath_group<3><<<g, b, 0, e->stream>>>(ch, tl, e->d_links, parity, max_attempts, kp, e->d_sweep, e->d_accepts, e->d_error); break;
+        }
+        return cudaGetLastError();
+    }
+    const dim3 g((unsigned)e->n_half_tiles);
     switch (mu) {
-    case 0: k_su2_heatbath<0><<<g, b, 0, e->stream>>>(ch, tl, e->d_links, parity, max_attempts, kp, e->d_sweep, e->d_accepts, e->d_error); break;
-    case 1: k_su2_heatbath<1><<<g, b, 0, e->stream>>>(ch, tl, e->d_links, parity, max_attempts, kp, e->d_sweep, e->d_accepts, e->d_error); break;
-    case 2: k_su2_heatbath<2><<<g, b, 0, e->stream>>>(ch, tl, e->d_links, parity, max_attempts, kp, e->d_sweep, e->d_accepts, e->d_error); break;
-    default: k_su2_heatbath<3><<<g, b, 0, e->stream>>>(ch, tl, e->d_links, parity, max_attempts, kp, e->d_sweep, e->d_accepts, e->d_error); break;
+    case 0: k_su2_heatbath_thread<0><<<g, b, 0, e->stream>>>(ch, tl, e->d_links, parity, max_attempts, kp, e->d_sweep, e->d_accepts, e->d_error); break;
+    case 1: k_su2_heatbath_thread<1><<<g, b, 0, e->stream>>>(ch, tl, e->d_links, parity, max_attempts, kp, e->d_sweep, e->d_accepts, e->d_error); break;
+    case 2: k_su2_heatbath_thread<2><<<g, b, 0, e->stream>>>(ch, tl, e->d_links, parity, max_attempts, kp, e->d_sweep, e->d_accepts, e->d_error); break;
+    default: k_su2_heatbath_thread<3><<<g, b, 0, e->stream>>>(ch, tl, e->d_links, parity, max_attempts, kp, e->d_sweep, e->d_accepts, e->d_error); break;
     }
     return cudaGetLastError();
 }
 
 cudaError_t launch_su2_overrelax(ym_ensemble *e, int parity, int mu) {
-    const dim3 g((unsigned)e->n_half_tiles), b(T);
     auto *ch = e->d_chains;
     auto *tl = e->d_half_tiles;
+    const dim3 b(T);
+    if (su2_grouped(e)) {
+        const dim3 g((unsigned)(e->n_half_tiles * kGroup));
+        switch (mu) {
+        case 0: k_su2_overrelax_group<0><<<g, b, 0, e->stream>>>(ch, tl, e->d_links, parity, e->d_error); break;
+        case 1: k_su2_overrelax_group<1><<<g, b, 0, e->stream>>>(ch, tl, e->d_links, parity, e->d_error); break;
+        case 2: k_su2_overrelax_group<2><<<g, b, 0, e->stream>>>(ch, tl, e->d_links, parity, e->d_error); break;
+        default: k_su2_overrelax_group<3><<<g, b, 0, e->stream>>>(ch, tl, e->d_links, parity, e->d_error); break;
+        }
+        return cudaGetLastError();
+    }
+    const dim3 g((unsigned)e->n_half_tiles);
     switch (mu) {
-    case 0: k_su2_overrelax<0><<<g, b, 0, e->stream>>>(ch, tl, e->d_links, parity, e->d_error); break;
-    case 1: k_su2_overrelax<1><<<g, b, 0, e->stream>>>(ch, tl, e->d_links, parity, e->d_error); break;
-    case 2: k_su2_overrelax<2><<<g, b, 0, e->stream>>>(ch, tl, e->d_links, parity, e->d_error); break;
-    default: k_su2_overrelax<3><<<g, b, 0, e->stream>>>(ch, tl, e->d_links, parity, e->d_error); break;
+    case 0: k_su2_overrelax_thread<0><<<g, b, 0, e->stream>>>(ch, tl, e->d_links, parity, e->d_error); break;
+    case 1: k_su2_overrelax_thread<1><<<g, b, 0, e->stream>>>(ch, tl, e->d_links, parity, e->d_error); break;
+    case 2: k_su2_overrelax_thread<2><<<g, b, 0, e->stream>>>(ch, tl, e->d_links, parity, e->d_error); break;
+    default: k_su2_overrelax_thread<3><<<g, b, 0, e->stream>>>(ch, tl, e->d_links, parity, e->d_error); break;
     }
     return cudaGetLastError();
 }
