@@ -76,6 +76,28 @@ def test_heatbath_matches_oracle_within_ulps(oracle):
     assert abs(plaq - ref) <= 1e-12
 
 
+@pytest.mark.parametrize("sampler", ["reference", "kennedy-pendleton"])
+def test_grouped_and_per_thread_kernels_agree(oracle, sampler):
+    """Small sub-sweeps run eight lanes per link, large ones one thread per
+    link (the switch is at 96 links per SM): the same chain, alone and as one
+    of 120 copies with the same seed, ends bit for bit the same."""
+    import ymgpu
+    ext = [4, 4, 4, 6]
+    start = rough(oracle, ext, 21)
+    seed = oracle.derive_chain_seed(0x2B0020121116_0101, 3)
+    out = []
+    for n in (1, 120):
+        with ymgpu.Ensemble([ext] * n, 2.3, [seed] * n, group=ymgpu.SU2) as ens:
+            for k in range(n):
+                ens.upload(k, start)
+            ens.markov_sweeps(3, overrelaxation_sweeps=2, max_attempts_per_link=10000, sampler=sampler)
+            prop, _ = ens.heatbath_accounting()
+            out.append((ens.download(0), ens.download(n - 1), int(prop[0]), int(prop[n - 1])))
+    (a0, _, pa, _), (b0, b1, pb0, pb1) = out
+    assert np.array_equal(a0, b0) and np.array_equal(a0, b1)
+    assert pa == pb0 == pb1
+
+
 def test_attempt_limit_fails_closed():
     """A bounded sampler that gives up reports HeatbathAttemptLimitExceeded
     (su2_ensemble.rs:229-253) instead of waiting."""

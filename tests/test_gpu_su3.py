@@ -87,6 +87,49 @@ def test_checkerboard_sweeps_bitwise_equal_oracle(oracle, uniform):
     assert np.array_equal(gpu, cpu)
 
 
+@pytest.mark.parametrize("uniform", [False, True])
+def test_batch_size_does_not_change_a_chain(oracle, uniform):
+    """One 4^4 chain alone (128 links per launch) and as one of 120 copies
+    with the same seed (15,360 links per launch) ends bit for bit on the
+    oracle's result."""
+    import ymgpu
+    ext = [4, 4, 4, 4]
+    start = rough_config(oracle, ext, 6)
+    seed = oracle.derive_su3_chain_seed(MASTER, 9)
+    mode = "uniform" if uniform else "ordered"
+    got = []
+    for n in (1, 120):
+        with ymgpu.Ensemble([ext] * n, 6.0, [seed] * n) as ens:
+            ens.sweep_path = "tiled"
+            for k in range(n):
+                ens.upload(k, start)
+            ens.metropolis_sweeps(0.3, 2, mode)
+            got.append((ens.download(0), ens.download(n - 1), int(ens.accounting()[1][0])))
+    cpu = start.copy()
+    na = 0
+    for sw in range(2):
+        na += oracle.su3_cb_sweep(ext, cpu, 6.0, 0.3, seed, sw, uniform)[1]
+    (a0, _, acc_a), (b0, b1, acc_b) = got
+    assert np.array_equal(a0, cpu) and np.array_equal(b0, cpu) and np.array_equal(b1, cpu)
+    assert acc_a == acc_b == na
+
+
+@pytest.mark.parametrize("path", ["tiled", "auto"])
+def test_measured_series_survives_a_larger_request(path):
+    """A measurement call asking for more rows than the last one grows the
+    series buffer; the captured measurement graph must then write into the
+    new buffer (every row filled, the last one the lattice's plaquette)."""
+    import ymgpu
+    with ymgpu.Ensemble([[4, 4, 4, 4]] * 2, 6.0, [3, 4]) as ens:
+        ens.sweep_path = path
+        ens.metropolis_sweeps(1.0, 20, "uniform")
+        first = ens.measured_sweeps(0.3, 5, 1, "uniform")
+        second = ens.measured_sweeps(0.3, 40, 1, "uniform")
+        last = ens.average_plaquette()
+    assert np.all(first > 0.2) and np.all(second > 0.2)
+    assert np.array_equal(second[-1], last)
+
+
 def test_graph_replay_equals_direct_launches(oracle):
     """Batches of >= 8 sweeps replay a captured CUDA graph; the device sweep
     counter advances on every replay, so 20 sweeps (2 replays + 4 direct)

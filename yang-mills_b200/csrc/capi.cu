@@ -545,6 +545,29 @@ int32_t ym_su3_metropolis_sweeps(ym_ensemble *e, double angle, int32_t generator
     return YM_OK;
 }
 
+}  // extern "C"
+
+// The per-measurement plaquette series buffer (rows x chains) and its device
+// row counter.  The captured measurement graph stores into d_series by
+// address, so growing the buffer also drops that graph: a graph replayed
+// after the reallocation would write into the freed buffer.
+static cudaError_t ensure_series(ym_ensemble *e, int64_t n_measurements) {
+    if (e->series_capacity < n_measurements) {
+        if (e->measure_graph) cudaGraphExecDestroy(e->measure_graph);
+        e->measure_graph = nullptr;
+        if (e->d_series) cudaFree(e->d_series);
+        e->d_series = nullptr;
+        e->series_capacity = 0;
+        cudaError_t err = dalloc(&e->d_series, (size_t)(n_measurements * e->n_chains));
+        if (err != cudaSuccess) return err;
+        e->series_capacity = n_measurements;
+    }
+    if (!e->d_series_row) return dalloc(&e->d_series_row, 1);
+    return cudaSuccess;
+}
+
+extern "C" {
+
 int32_t ym_su3_measured_sweeps(ym_ensemble *e, double angle, int32_t generator_mode,
                                int64_t n_measurements, int64_t sweeps_per_measurement,
                                double *series) {
@@ -561,14 +584,7 @@ int32_t ym_su3_measured_sweeps(ym_ensemble *e, double angle, int32_t generator_m
     st = set_device(e);
     if (st) return st;
     if (n_measurements == 0) return YM_OK;
-    if (e->series_capacity < n_measurements) {
-        if (e->d_series) cudaFree(e->d_series);
-        e->d_series = nullptr;
-        e->series_capacity = 0;
-        YM_CUDA(dalloc(&e->d_series, (size_t)(n_measurements * e->n_chains)));
-        e->series_capacity = n_measurements;
-    }
-    if (!e->d_series_row) YM_CUDA(dalloc(&e->d_series_row, 1));
+    YM_CUDA(ensure_series(e, n_measurements));
     YM_CUDA(cudaMemsetAsync(e->d_series_row, 0, sizeof(uint64_t), e->stream));
     auto step = [&]() -> cudaError_t {
         for (int64_t k = 0; k < sweeps_per_measurement; ++k) {
@@ -1372,14 +1388,7 @@ int32_t ym_su3_learned_measured_sweeps(ym_ensemble *e, ym_proposal_model *m, int
     st = set_device(e);
     if (st) return st;
     YM_CUDA(cudaStreamSynchronize(m->stream));
-    if (e->series_capacity < n_measurements) {
-        if (e->d_series) cudaFree(e->d_series);
-        e->d_series = nullptr;
-        e->series_capacity = 0;
-        YM_CUDA(dalloc(&e->d_series, (size_t)(n_measurements * e->n_chains)));
-        e->series_capacity = n_measurements;
-    }
-    if (!e->d_series_row) YM_CUDA(dalloc(&e->d_series_row, 1));
+    YM_CUDA(ensure_series(e, n_measurements));
     YM_CUDA(cudaMemsetAsync(e->d_series_row, 0, sizeof(uint64_t), e->stream));
     for (int64_t meas = 0; meas < n_measurements; ++meas) {
         for (int64_t k = 0; k < sweeps_per_measurement; ++k) YM_CUDA(learned_sweep(e, m));

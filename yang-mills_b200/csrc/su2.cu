@@ -133,24 +133,6 @@ __device__ __forceinline__ q4 qdag_if(const q4 &a, bool d) {
     return q4{{a.c[0], s * a.c[1], s * a.c[2], s * a.c[3]}};
 }
 
-__device__ __forceinline__ int32_t coord_of(const int32_t *x, int d) {
-    return d == 0 ? x[0] : (d == 1 ? x[1] : (d == 2 ? x[2] : x[3]));
-}
-
-// Neighbour along a direction chosen per lane (selects, no indexed arrays).
-__device__ __forceinline__ Nb step_any(const ChainInfo &c, const int32_t *x, int64_t lex, int par,
-                                       int d, int dir) {
-    const int32_t xd = coord_of(x, d), nd = coord_of(c.n, d);
-    const int64_t st = d == 3 ? 1 : (d == 2 ? (int64_t)c.n[3]
-                                            : (d == 1 ? (int64_t)c.n[2] * c.n[3]
-                                                      : (int64_t)c.n[1] * c.n[2] * c.n[3]));
-    const bool wrap = dir > 0 ? (xd == nd - 1) : (xd == 0);
-    const int64_t nl = dir > 0 ? (wrap ? lex - (int64_t)(nd - 1) * st : lex + st)
-                               : (wrap ? lex + (int64_t)(nd - 1) * st : lex - st);
-    const int flip = (wrap && (nd & 1)) ? 0 : 1;
-    return Nb{nl, par ^ flip};
-}
-
 // Term j of the staple of link (x, MU):
 //   forward  U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag
 //   backward U_nu(x-nu+mu)^dag U_mu(x-nu)^dag U_nu(x-nu)

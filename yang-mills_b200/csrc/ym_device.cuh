@@ -327,6 +327,26 @@ __device__ __forceinline__ Nb step(const ChainInfo &c, const int32_t *x, int64_t
     return Nb{shift_lex(c, x, lex, d, dir), par ^ flip};
 }
 
+__device__ __forceinline__ int32_t coord_of(const int32_t *x, int d) {
+    return d == 0 ? x[0] : (d == 1 ? x[1] : (d == 2 ? x[2] : x[3]));
+}
+
+// step() for a direction chosen per thread at run time: the coordinate and
+// stride are picked with selects, so no array is indexed dynamically (a
+// dynamically indexed coordinate array would live in local memory).
+__device__ __forceinline__ Nb step_any(const ChainInfo &c, const int32_t *x, int64_t lex, int par,
+                                       int d, int dir) {
+    const int32_t xd = coord_of(x, d), nd = coord_of(c.n, d);
+    const int64_t st = d == 3 ? 1 : (d == 2 ? (int64_t)c.n[3]
+                                            : (d == 1 ? (int64_t)c.n[2] * c.n[3]
+                                                      : (int64_t)c.n[1] * c.n[2] * c.n[3]));
+    const bool wrap = dir > 0 ? (xd == nd - 1) : (xd == 0);
+    const int64_t nl = dir > 0 ? (wrap ? lex - (int64_t)(nd - 1) * st : lex + st)
+                               : (wrap ? lex + (int64_t)(nd - 1) * st : lex - st);
+    const int flip = (wrap && (nd & 1)) ? 0 : 1;
+    return Nb{nl, par ^ flip};
+}
+
 // SU(3) FP64 link access: plane (mu*9 + entry) of a chain's block.
 __device__ __forceinline__ m3 load_su3(const double2 *__restrict__ links, const ChainInfo &c,
                                        int64_t s, int mu) {
