@@ -34,23 +34,6 @@ struct Walker {
     int par;
 };
 
-// a * b with every entry one fixed chain of fma() over k = 0, 1, 2: half the
-// FP64 instructions of mul, for the loop measurements that are held to
-// 1e-12 relative rather than bitwise.
-__device__ __forceinline__ m3 mul_fma(const m3 &a, const m3 &b) {
-    m3 o;
-#pragma unroll
-    for (int r = 0; r < 3; ++r)
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            cplx v = cmake(0.0, 0.0);
-#pragma unroll
-            for (int k = 0; k < 3; ++k) cfma(v, a.e[r][k], b.e[k][c]);
-            o.e[r][c] = v;
-        }
-    return o;
-}
-
 __device__ __forceinline__ Walker walker_of(const Coord &x) {
     Walker w;
 #pragma unroll

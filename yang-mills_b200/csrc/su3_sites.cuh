@@ -43,7 +43,10 @@ __device__ __forceinline__ double block_reduce(double v) {
 
 // Sum over the six planes of (1/3) Re Tr of the site's plaquettes, in the
 // order (mu, nu) = (0,1),(0,2),(0,3),(1,2),(1,3),(2,3); each product in the
-// reference's orientation U_mu(x) U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag.
+// reference's orientation U_mu(x) U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag, its
+// two matrix products as fma() chains (within 1e-12 relative of the
+// reference's plaquette; the tiled and chain-resident paths share this code
+// and so agree bitwise).
 template <bool RESIDENT>
 __device__ __forceinline__ double site_plaquette_sum(const double2 *links, const ChainInfo &c,
                                                      int64_t s) {
@@ -57,8 +60,8 @@ __device__ __forceinline__ double site_plaquette_sum(const double2 *links, const
 #pragma unroll 1
         for (int nu = mu + 1; nu < 4; ++nu) {
             const Nb pn = step(c, x.x, x.lex, x.par, nu, +1);
-            m3 p = mul(umu, link_at<RESIDENT>(links, c, storage_index(c, pm.lex, pm.par), nu));
-            p = mul_adj(p, link_at<RESIDENT>(links, c, storage_index(c, pn.lex, pn.par), mu));
+            m3 p = mul_fma(umu, link_at<RESIDENT>(links, c, storage_index(c, pm.lex, pm.par), nu));
+            p = mul_adj_fma(p, link_at<RESIDENT>(links, c, storage_index(c, pn.lex, pn.par), mu));
             const double val = retrace_mul_adj(p, link_at<RESIDENT>(links, c, s, nu)) / 3.0;
             v = first ? val : v + val;
             first = false;
