@@ -147,7 +147,7 @@ __device__ __forceinline__ void wilson_site(const double2 *links, const ChainInf
     }
 }
 
-__global__ void __launch_bounds__(T, 3)
+__global__ void __launch_bounds__(T)
 k_wilson_loops(const ChainInfo *__restrict__ chains, const Tile *__restrict__ tiles,
                const double2 *__restrict__ links, int rmax, int tmax, double *__restrict__ partial) {
     extern __shared__ __align__(16) double2 qs[];
