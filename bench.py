@@ -379,8 +379,16 @@ def main():
         return {"ms": o_s * 1e3, "calls_timed": o_n, "compulsory_bytes": o_bytes,
                 "achieved_gbs": o_bytes / o_s / 1e9, "frac": o_bytes / o_s / 1e9 / peak}
 
+    wilson = obs_leg("aux", lambda: ens.wilson_loops(4, 4), 4)
+    # its arithmetic: per site and plane 38 3x3 complex products (D_T, A_R,
+    # P_{R,T}, Q_{R,T} for R, T <= 4), each 9 entries x 3 complex fma =
+    # 216 flops, so 8,208 flops (the 16 traces not counted); the ratio is to
+    # the B200's nominal 37 TFLOP/s FP64 (no measured FP64 peak exists here)
+    w_flops = volume * 6 * 38 * 216
+    wilson.update({"fp64_tflops": w_flops / (wilson["ms"] * 1e-3) / 1e12,
+                   "fp64_frac_of_nominal_37": w_flops / (wilson["ms"] * 1e-3) / 37e12})
     observables = {
-        "wilson_loops_4x4_all_planes": obs_leg("aux", lambda: ens.wilson_loops(4, 4), 4),
+        "wilson_loops_4x4_all_planes": wilson,
         "polyakov_loop_dir3": obs_leg("aux", lambda: ens.polyakov_loops(3), 1),
         "a1pp_operator_basis": obs_leg("operators", ens.scalar_operator_basis, 3),
         "peak_gbs": peak, "peak_source": f"{peak_kind} hbm_gbs",
