@@ -338,6 +338,18 @@ def su3_staple(extents, links, x, mu) -> np.ndarray:
     return out
 
 
+def su3_visit(u, a, beta, angle, key, uniform_generator=False):
+    """One link visit of the checkerboard sweep (or_b200.c su3_visit): U after
+    its eight hits given the staple sum A and the link's stream key, and the
+    number of accepted hits."""
+    uu = np.ascontiguousarray(u, np.complex128).copy()
+    aa = np.ascontiguousarray(a, np.complex128)
+    acc = u64()
+    _check(lib().or_su3_visit(_dp(uu.view(np.float64)), _dp(aa.view(np.float64)), beta, angle,
+                              key, int(uniform_generator), C.byref(acc)), "su3_visit")
+    return uu, acc.value
+
+
 def su3_cb_sweep(extents, links, beta, angle, chain_seed, sweep, uniform_generator=False):
     p, a = u64(), u64()
     _check(lib().or_su3_cb_sweep(_ext(extents), _dp(links.view(np.float64)), beta, angle,
