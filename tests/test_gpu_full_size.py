@@ -8,6 +8,8 @@ the oracle to sweep the whole lattice.
   later ones at their pre-sweep values — and must equal the GPU's links bit
   for bit; the lattice plaquette matches the oracle's sequential sum to
   1e-12 relative and the links stay in SU(3) to 1e-12.
+* 32^4 two-row FP32: one sweep from the same field, seed and sweep index as
+  the FP64 sweep stays within the FP32 path's stated error of it.
 * SU(2) 10^4 at beta 2.3 (the heat-bath workload): the GPU sweep equals the
   oracle's checkerboard sweep (overrelaxation bitwise, heat-bath to 1e-12).
 * 64 chains of 4^4 (the batched-chain workload): chains across the batch
@@ -101,6 +103,32 @@ def test_full_size_sweep_sampled_links_bitwise(oracle, ext, uniform):
     ref = oracle.su3_average_plaquette(ext, after)
     assert abs(plaq - ref) <= 1e-12 * abs(ref)
     assert ures[0] <= 1e-12 and dres[0] <= 1e-12
+
+
+def test_full_size_fp32_sweep_error_against_fp64(oracle):
+    """The two-row binary32 sweep at 32^4, from the same field, seed and sweep
+    index as the FP64 sweep (bitwise the oracle's, above): >= 98% of links
+    within 1e-5 of the FP64 result (a decision may flip where the uniform
+    lies within the ~1e-6 dS error of exp(-dS)), plaquettes within 1e-6."""
+    import ymgpu
+    ext = [32, 32, 32, 32]
+    seed = oracle.derive_su3_chain_seed(MASTER, 5)
+    with ymgpu.Ensemble([ext], 6.0, seed, lift_reference_caps=True) as e64, \
+            ymgpu.Ensemble([ext], 6.0, seed, precision=ymgpu.F32_TWO_ROW,
+                           lift_reference_caps=True) as e32:
+        e64.hot_start()
+        e64.metropolis_sweeps(1.0, 3, "uniform")
+        e32.upload(0, e64.download(0))
+        e32.sweep_index = e64.sweep_index
+        e64.metropolis_sweeps(0.3, 1)
+        e32.metropolis_sweeps(0.3, 1)
+        a = e64.download(0)
+        b = e32.download(0)
+        p64 = e64.average_plaquette()[0]
+        p32 = e32.average_plaquette()[0]
+    per_link = np.abs(a - b).reshape(len(a), -1).max(1)
+    assert np.mean(per_link <= 1e-5) >= 0.98
+    assert abs(p64 - p32) <= 1e-6
 
 
 def test_su2_10x4_sweep_equals_oracle(oracle):
