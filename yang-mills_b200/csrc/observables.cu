@@ -69,7 +69,7 @@ __device__ __forceinline__ void block_sum16(double v[16], double *out) {
 //   Q_{R,T} = U_nu(x)..U_nu(x+(T-1)nu) U_mu(x+T nu)..U_mu(x+T nu+(R-1)mu)
 // each multiplied left to right in traversal order (fma chains); P grows in T from the
 // mu-line A_R, Q grows in R (Q_{0,T} = the nu-line D_T), so all sixteen loops
-// take 39 products instead of 160.  The four Q_{R-1,T} wait in shared memory
+// take 38 products instead of 160.  The four Q_{R-1,T} wait in shared memory
 // between R steps.  Re (1/3) Tr(P Q^dag) differs from the single-chain
 // product only by rounding (<= 1e-12 relative on lattice means).
 // partial[(tile * 6 + plane) * 16 + (R-1)*4 + (T-1)] = tile sum.
