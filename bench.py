@@ -88,7 +88,7 @@ def measured_peaks():
 def ncu_traffic_per_launch():
     """DRAM bytes per k_su3_metropolis launch from the committed ncu summary,
     scaled to a 32^4 launch (None when no summary exists)."""
-    path = os.path.join(ROOT, "profiles", "su3_metropolis_f64.md")
+    path = os.path.join(ROOT, "profiles", "su3_metropolis_32x4_fp64.md")
     try:
         for line in open(path):
             if line.startswith("dram_bytes_per_32^4_launch:"):
