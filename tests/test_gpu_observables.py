@@ -47,6 +47,31 @@ def test_wilson_loops_match_oracle_site_sums(oracle):
     assert np.all(w[:, 3, :] == 0.0) and np.all(w[:, :, 2:] == 0.0)
 
 
+def test_loops_on_an_uneven_batch(oracle):
+    """Chains of different extents in one handle: each chain's Wilson-loop
+    and Polyakov-loop means (per-chain tile sums, one thread per Polyakov
+    line) match the oracle to 1e-12."""
+    import ymgpu
+    exts = [[4, 4, 2, 4], [2, 4, 6, 8], [6, 2, 2, 4]]
+    starts = [rough(oracle, e, 50 + i) for i, e in enumerate(exts)]
+    with ymgpu.Ensemble(exts, 6.0, [1, 2, 3]) as ens:
+        for i, st in enumerate(starts):
+            ens.upload(i, st)
+        w = ens.wilson_loops(2, 2)
+        pol = {d: ens.polyakov_loops(d) for d in range(4)}
+    for i, e in enumerate(exts):
+        sites = list(site_iter(e))
+        for p, (mu, nu) in enumerate(PLANES):
+            for r in (1, 2):
+                for t in (1, 2):
+                    steps = oracle.rectangular_path(mu, nu, r, t)
+                    ref = np.mean([oracle.su3_wilson_loop(e, starts[i], x, steps).real for x in sites])
+                    assert abs(w[i, p, r - 1, t - 1] - ref) <= 1e-12 * max(1.0, abs(ref)), (i, p, r, t)
+        for d in range(4):
+            ref = np.mean([oracle.su3_polyakov_loop(e, starts[i], x, d) for x in sites if x[d] == 0])
+            assert abs(pol[d][i] - ref) <= 1e-12, (i, d)
+
+
 def test_polyakov_loop_matches_oracle(oracle):
     import ymgpu
     ext = [4, 2, 4, 6]
