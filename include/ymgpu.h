@@ -165,8 +165,10 @@ int32_t ym_su2_max_unit_residual(ym_ensemble *ens, double *per_chain);
 
 /* ---- observables ----
  * Average plaquette per chain (su3_ensemble.rs:228 / su2_ensemble.rs:348):
- * mean over sites and mu<nu of (1/N) Re Tr P, FP64 tree reduction in a fixed
- * order (deterministic; within 1e-15 relative of the sequential sum). */
+ * mean over sites and mu<nu of (1/N) Re Tr P, each SU(3) plaquette's two
+ * matrix products as fma chains, FP64 tree reduction in a fixed order
+ * (deterministic; within 1e-12 relative of the reference's sequential sum,
+ * tested up to 32^4). */
 int32_t ym_average_plaquette(ym_ensemble *ens, double *per_chain);
 /* Average plaquette without any device allocation.  No counterpart in the
  * reference: it serves callers that cannot allocate device memory (a host
@@ -197,7 +199,9 @@ int32_t ym_su3_average_plaquette_noalloc(const double *links, const int64_t *ext
  * Re wilson_loop(x, rectangular_path(mu, nu, R, T)) (path_holonomy.rs:172-260;
  * R steps along mu, T along nu).  out[((chain*6 + plane)*4 + R-1)*4 + T-1];
  * entries beyond (rmax, tmax) are 0.  The lattice average has no reference
- * counterpart; each per-site value is the reference's primitive. */
+ * counterpart; each per-site value is the reference's primitive, evaluated
+ * as Re Tr of the closed path's two halves (agreeing with the reference's
+ * single left-to-right product to rounding; means within 1e-12). */
 int32_t ym_su3_wilson_loops(ym_ensemble *ens, int32_t rmax, int32_t tmax, double *out);
 /* Polyakov loop (su3_lattice.rs:185-212) averaged over every start site with
  * x_dir = 0: out[chain*2 + 0] = mean Re, out[chain*2 + 1] = mean Im. */
