@@ -219,6 +219,11 @@ int32_t ym_ensemble_copy(ym_ensemble *src, ym_ensemble *dst);
  * of another handle (device to device). */
 int32_t ym_ensemble_copy_chain(ym_ensemble *src, int64_t src_chain, ym_ensemble *dst,
                                int64_t dst_chain);
+/* The same for `count` consecutive chains (src_first.. into dst_first..),
+ * each pair of equal extents: chains of a handle are laid out back to back,
+ * so this is one device-to-device copy and one synchronisation. */
+int32_t ym_ensemble_copy_chains(ym_ensemble *src, int64_t src_first, ym_ensemble *dst,
+                                int64_t dst_first, int64_t count);
 /* spatial_stout_smear (glueball_smearing.rs:257-268): `levels` synchronous
  * spatial stout levels of src written to dst (same extents); rho in
  * (0, 0.25], levels <= 8 unless lift_level_cap (sequential levels compose,

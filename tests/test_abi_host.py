@@ -103,6 +103,29 @@ def test_config_validation_fails_closed():
     Su3EnsembleConfig(**{**base, "extents": [32, 32, 32, 32]}).validate(lift_reference_caps=True)
 
 
+def test_jackknife_replicas_every_replica_and_failures(oracle):
+    """Every delete-one replica (computed on the host's threads from shared
+    products) equals the one-replica function bit for bit, and a rejected
+    input returns the status the one-at-a-time loop returns."""
+    from ymgpu import glueball as G
+    from ymgpu.errors import YmError
+    rng = np.random.default_rng(11)
+    s = rng.normal(0.9, 0.02, size=(300, 12))
+    reps = G.jackknife_replicas(s)
+    for k in range(300):
+        assert np.array_equal(reps[k], G.connected_from_samples(s, k)), k
+    for k in (0, 149, 299):
+        assert np.array_equal(reps[k], oracle.connected_from_samples(s, k))
+    bad = s.copy()
+    bad[5, 3] = np.nan
+    with pytest.raises(YmError) as e:
+        G.jackknife_replicas(bad)
+    assert e.value.variant == "NonFiniteStatistic"
+    with pytest.raises(YmError) as e:
+        G.jackknife_replicas(s[:1])
+    assert e.value.variant == "EmptyConfigurationSet"
+
+
 def test_host_correlators_equal_oracle(oracle, golden):
     """Connected correlators, delete-one jackknife and covariance: the
     library's host FP64 code equals the oracle bit for bit."""

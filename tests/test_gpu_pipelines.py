@@ -56,3 +56,30 @@ def test_uneven_glueball_pipeline(oracle):
         assert np.array_equal(s.plaquette_connected,
                               oracle.connected_from_samples(s.plaquette_samples))
     assert res.link_updates == (3 * 384 + 2 * 864) * 4 * (6 + 2 * 2)
+
+
+def test_copy_of_consecutive_chains(oracle):
+    """ym_ensemble_copy_chains copies a run of chains (uneven extents) in one
+    device copy; mismatched extents or ranges fail closed."""
+    import ymgpu
+    from ymgpu.errors import YmError
+    exts = [[4, 4, 4, 4], [2, 4, 6, 8], [4, 4, 2, 6], [4, 4, 4, 4]]
+    with ymgpu.Ensemble(exts, 6.0, [1, 2, 3, 4]) as src:
+        src.hot_start()
+        with ymgpu.Ensemble(exts[1:3], 6.0, [0, 0]) as dst:
+            src.copy_chains_to(1, dst, 0, 2)
+            assert np.array_equal(dst.download(0), src.download(1))
+            assert np.array_equal(dst.download(1), src.download(2))
+            with pytest.raises(YmError) as e:
+                src.copy_chains_to(0, dst, 0, 2)
+            assert e.value.variant == "LatticeExtentsMismatch"
+            with pytest.raises(YmError) as e:
+                src.copy_chains_to(3, dst, 0, 2)
+            assert e.value.variant == "InvalidArgument"
+        sub = src.subset([0, 1, 3])
+        try:
+            for j, c in enumerate([0, 1, 3]):
+                assert np.array_equal(sub.download(j), src.download(c))
+        finally:
+            sub.close()
+

@@ -857,6 +857,36 @@ int32_t ym_ensemble_copy_chain(ym_ensemble *src, int64_t src_chain, ym_ensemble 
     return YM_OK;
 }
 
+int32_t ym_ensemble_copy_chains(ym_ensemble *src, int64_t src_first, ym_ensemble *dst,
+                                int64_t dst_first, int64_t count) {
+    if (!src || !dst) return YM_ERR_NULL_ARGUMENT;
+    if (count < 0 || src_first < 0 || dst_first < 0 || src_first > src->n_chains - count ||
+        dst_first > dst->n_chains - count)
+        return YM_ERR_INVALID_ARGUMENT;
+    if (count == 0) return YM_OK;
+    if (src->group != dst->group || src->precision != dst->precision || src->device != dst->device)
+        return YM_ERR_LATTICE_EXTENTS_MISMATCH;
+    for (int64_t i = 0; i < count; ++i) {
+        const ChainInfo &a = src->chains[src_first + i], &b = dst->chains[dst_first + i];
+        for (int d = 0; d < 4; ++d)
+            if (a.n[d] != b.n[d]) return YM_ERR_LATTICE_EXTENTS_MISMATCH;
+    }
+    int32_t st = set_device(dst);
+    if (st) return st;
+    const size_t elem = f32(src) ? sizeof(float2) : sizeof(double2);
+    const size_t per_link = f32(src) ? 6 : (src->group == YM_GROUP_SU3 ? 9 : 2);
+    const ChainInfo &first = src->chains[src_first], &last = src->chains[src_first + count - 1];
+    // chains sit back to back (offset of chain k+1 = offset of k + its size)
+    const size_t bytes = (size_t)(last.offset - first.offset) * elem +
+                         (size_t)last.volume * 4 * per_link * elem;
+    YM_CUDA(cudaStreamSynchronize(src->stream));
+    YM_CUDA(cudaMemcpyAsync(reinterpret_cast<char *>(dst->d_links) + (size_t)dst->chains[dst_first].offset * elem,
+                            reinterpret_cast<const char *>(src->d_links) + (size_t)first.offset * elem,
+                            bytes, cudaMemcpyDeviceToDevice, dst->stream));
+    YM_CUDA(cudaStreamSynchronize(dst->stream));
+    return YM_OK;
+}
+
 int32_t ym_su3_spatial_stout_smear(ym_ensemble *src, ym_ensemble *dst, double rho, int64_t levels,
                                    int32_t lift_level_cap) {
     if (!src || !dst) return YM_ERR_NULL_ARGUMENT;

@@ -5,8 +5,10 @@
 // kernels so that run_chain-style callers get the reference's numbers.
 // Compiled with -ffp-contract=off: every sum is left to right as in the
 // reference's iterator chains.
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <thread>
 #include <vector>
 
 #include "../../include/ymgpu.h"
@@ -244,13 +246,86 @@ int32_t ym_connected_from_samples(const double *samples, int64_t ncfg, int64_t n
     return YM_OK;
 }
 
+// Every delete-one replica of ym_connected_from_samples.  Each replica's
+// sums run in that function's order (configurations ascending, t ascending,
+// the omitted one skipped) over the same rounded products, so every value is
+// its bits; the products row[t] * row[(t + tau) % nt] are formed once for all
+// replicas and the replicas are spread over the host's threads.  Inputs that
+// the function would reject (a non-finite sample, fewer than two
+// configurations) take the one-replica-at-a-time path, which returns the
+// first failing replica's status exactly as before.
 int32_t ym_jackknife_replicas(const double *samples, int64_t ncfg, int64_t nt, double *replicas) {
     if (!samples || !replicas) return YM_ERR_NULL_ARGUMENT;
-    for (int64_t k = 0; k < ncfg; ++k) {
-        const int32_t st = ym_connected_from_samples(samples, ncfg, nt, k, replicas + k * nt);
-        if (st) return st;
+    bool plain = ncfg < 2 || nt <= 0 || ncfg > (((int64_t)1 << 40) / std::max<int64_t>(nt, 1));
+    for (int64_t i = 0; !plain && i < ncfg * nt; ++i)
+        if (!std::isfinite(samples[i])) plain = true;
+    if (plain) {
+        for (int64_t k = 0; k < ncfg; ++k) {
+            const int32_t st = ym_connected_from_samples(samples, ncfg, nt, k, replicas + k * nt);
+            if (st) return st;
+        }
+        return ncfg > 0 ? YM_OK : YM_ERR_EMPTY_CONFIGURATION_SET;
     }
-    return ncfg > 0 ? YM_OK : YM_ERR_EMPTY_CONFIGURATION_SET;
+    // products[(c * nt + tau) * nt + t], kept while they fit in 256 MB
+    std::vector<double> products;
+    if (ncfg * nt * nt <= ((int64_t)1 << 25)) {
+        products.resize((size_t)(ncfg * nt * nt));
+        for (int64_t c = 0; c < ncfg; ++c) {
+            const double *row = samples + c * nt;
+            for (int64_t tau = 0; tau < nt; ++tau)
+                for (int64_t t = 0; t < nt; ++t)
+                    products[(size_t)((c * nt + tau) * nt + t)] = row[t] * row[(t + tau) % nt];
+        }
+    }
+    std::vector<int32_t> status((size_t)ncfg, YM_OK);
+    auto replica = [&](int64_t k) {
+        const int64_t count = (ncfg - 1) * nt;
+        double ms = 0.0;
+        for (int64_t c = 0; c < ncfg; ++c) {
+            if (c == k) continue;
+            for (int64_t t = 0; t < nt; ++t) ms += samples[c * nt + t];
+        }
+        const double mean = ms / (double)count;
+        const double msq = mean * mean;
+        if (!std::isfinite(mean) || !std::isfinite(msq)) {
+            status[(size_t)k] = YM_ERR_NON_FINITE_STATISTIC;
+            return;
+        }
+        for (int64_t tau = 0; tau < nt; ++tau) {
+            double s = 0.0;
+            for (int64_t c = 0; c < ncfg; ++c) {
+                if (c == k) continue;
+                if (!products.empty()) {
+                    const double *pr = products.data() + (c * nt + tau) * nt;
+                    for (int64_t t = 0; t < nt; ++t) s += pr[t];
+                } else {
+                    const double *row = samples + c * nt;
+                    for (int64_t t = 0; t < nt; ++t) s += row[t] * row[(t + tau) % nt];
+                }
+            }
+            const double v = s / (double)count - msq;
+            if (!std::isfinite(v)) {
+                status[(size_t)k] = YM_ERR_NON_FINITE_STATISTIC;
+                return;
+            }
+            replicas[k * nt + tau] = v;
+        }
+    };
+    const int64_t hw = std::max<int64_t>(1, (int64_t)std::thread::hardware_concurrency());
+    const int64_t n_threads = std::min<int64_t>(hw, std::max<int64_t>(1, ncfg / 8));
+    if (n_threads <= 1) {
+        for (int64_t k = 0; k < ncfg; ++k) replica(k);
+    } else {
+        std::vector<std::thread> pool;
+        for (int64_t w = 0; w < n_threads; ++w)
+            pool.emplace_back([&, w] {
+                for (int64_t k = w; k < ncfg; k += n_threads) replica(k);
+            });
+        for (std::thread &th : pool) th.join();
+    }
+    for (int64_t k = 0; k < ncfg; ++k)
+        if (status[(size_t)k] != YM_OK) return status[(size_t)k];
+    return YM_OK;
 }
 
 // glueball_scalar_fit.rs:276-322

@@ -55,6 +55,7 @@ SIGNATURES = {
     "ym_su3_scalar_operator_basis": [VP, P(f64), P(f64)],
     "ym_ensemble_copy": [VP, VP],
     "ym_ensemble_copy_chain": [VP, i64, VP, i64],
+    "ym_ensemble_copy_chains": [VP, i64, VP, i64, i64],
     "ym_su3_spatial_stout_smear": [VP, VP, f64, i64, i32],
     "ym_su3_spatial_stride2_block": [VP, VP],
     "ym_periodic_connected_estimator": [P(f64), i64, i64, P(f64), P(f64), P(f64)],

@@ -251,14 +251,30 @@ class Ensemble:
     def copy_chain_to(self, chain: int, dst: "Ensemble", dst_chain: int) -> None:
         check(lib().ym_ensemble_copy_chain(self._h, chain, dst.handle, dst_chain), "copy_chain")
 
+    def copy_chains_to(self, first: int, dst: "Ensemble", dst_first: int, count: int) -> None:
+        """Copy chains first..first+count-1 into dst_first.. of dst (one copy)."""
+        check(lib().ym_ensemble_copy_chains(self._h, first, dst.handle, dst_first, count),
+              "copy_chains")
+
+    def copy_subset_to(self, chains, dst: "Ensemble") -> None:
+        """Copy the given chains into chains 0.. of dst, one copy per run of
+        consecutive chain indices."""
+        chains = list(chains)
+        j = 0
+        while j < len(chains):
+            k = j
+            while k + 1 < len(chains) and chains[k + 1] == chains[k] + 1:
+                k += 1
+            self.copy_chains_to(chains[j], dst, j, k - j + 1)
+            j = k + 1
+
     def subset(self, chains) -> "Ensemble":
         """A new handle holding a device copy of the given chains."""
         chains = list(chains)
         out = Ensemble([self.extents[c] for c in chains], self.beta[chains], self.seeds[chains],
                        group=self.group, precision=self.precision, lift_reference_caps=True,
                        device=self.device)
-        for j, c in enumerate(chains):
-            self.copy_chain_to(c, out, j)
+        self.copy_subset_to(chains, out)
         return out
 
     def copy_to(self, dst: "Ensemble") -> None:

@@ -149,8 +149,7 @@ def scalar_glueball_pipeline(groups: Sequence[Tuple[int, Sequence[int]]] = ((128
                     for gi, chains in enumerate(per_group):
                         samples.setdefault((gi, levels, False), []).extend(basis[c] for c in chains)
                         if gi in subs:
-                            for j, c in enumerate(chains):
-                                sm.copy_chain_to(c, subs[gi], j)
+                            sm.copy_subset_to(chains, subs[gi])
                             subs[gi].block_into(coarse[gi])
                             samples.setdefault((gi, levels, True), []).extend(
                                 coarse[gi].scalar_operator_basis())
