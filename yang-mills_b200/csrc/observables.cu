@@ -70,7 +70,8 @@ __device__ __forceinline__ void block_sum16(double v[16], double *out) {
 // each multiplied left to right in traversal order (fma chains); P grows in T from the
 // mu-line A_R, Q grows in R (Q_{0,T} = the nu-line D_T), so all sixteen loops
 // take 38 products instead of 160.  The four Q_{R-1,T} wait in shared memory
-// between R steps.  Re (1/3) Tr(P Q^dag) differs from the single-chain
+// between R steps, and the sixteen loop values are written straight to the
+// thread's shared-memory column (fewer registers than an indexed array).  Re (1/3) Tr(P Q^dag) differs from the single-chain
 // product only by rounding (<= 1e-12 relative on lattice means).
 // partial[(tile * 6 + plane) * 16 + (R-1)*4 + (T-1)] = tile sum.
 constexpr size_t kWilsonSmem = (size_t)kMaxRT * 9 * T * sizeof(double2);
@@ -104,7 +105,7 @@ __device__ __forceinline__ m3 q_get(const double2 *qs, int t) {
 
 template <int MU, int NU>
 __device__ __forceinline__ void wilson_site(const double2 *links, const ChainInfo &c, const Walker &w0,
-                                            int rmax, int tmax, double2 *qs, double v[16]) {
+                                            int rmax, int tmax, double2 *qs, double (*vs)[T]) {
     {   // D_T, stored as Q_{0,T}
         Walker w = w0;
         m3 d;
@@ -137,10 +138,7 @@ __device__ __forceinline__ void wilson_site(const double2 *links, const ChainInf
                     step_walker(c, wq, NU);
                     const m3 q = mul_fma(q_get(qs, t), link_of(links, c, wq, MU));
                     q_put(qs, t, q);
-                    const double val = retrace_mul_adj(p, q) * (1.0 / 3.0);
-#pragma unroll
-                    for (int k = 0; k < 16; ++k)
-                        if (k == r * kMaxRT + t) v[k] = val;
+                    vs[r * kMaxRT + t][threadIdx.x] = retrace_mul_adj(p, q) * (1.0 / 3.0);
                 }
             }
         }
@@ -151,24 +149,27 @@ __global__ void __launch_bounds__(T)
 k_wilson_loops(const ChainInfo *__restrict__ chains, const Tile *__restrict__ tiles,
                const double2 *__restrict__ links, int rmax, int tmax, double *__restrict__ partial) {
     extern __shared__ __align__(16) double2 qs[];
+    __shared__ double vs[16][T];
     const int plane = blockIdx.y;
     const Tile tile = tiles[blockIdx.x];
     const ChainInfo c = chains[tile.chain];
     const int64_t s = tile.start + threadIdx.x;
-    double v[16];
 #pragma unroll
-    for (int k = 0; k < 16; ++k) v[k] = 0.0;
+    for (int k = 0; k < 16; ++k) vs[k][threadIdx.x] = 0.0;
     if (s < c.volume) {
         const Walker w0 = walker_of(decode_storage(c, s));
         switch (plane) {
-            case 0: wilson_site<0, 1>(links, c, w0, rmax, tmax, qs, v); break;
-            case 1: wilson_site<0, 2>(links, c, w0, rmax, tmax, qs, v); break;
-            case 2: wilson_site<0, 3>(links, c, w0, rmax, tmax, qs, v); break;
-            case 3: wilson_site<1, 2>(links, c, w0, rmax, tmax, qs, v); break;
-            case 4: wilson_site<1, 3>(links, c, w0, rmax, tmax, qs, v); break;
-            default: wilson_site<2, 3>(links, c, w0, rmax, tmax, qs, v); break;
+            case 0: wilson_site<0, 1>(links, c, w0, rmax, tmax, qs, vs); break;
+            case 1: wilson_site<0, 2>(links, c, w0, rmax, tmax, qs, vs); break;
+            case 2: wilson_site<0, 3>(links, c, w0, rmax, tmax, qs, vs); break;
+            case 3: wilson_site<1, 2>(links, c, w0, rmax, tmax, qs, vs); break;
+            case 4: wilson_site<1, 3>(links, c, w0, rmax, tmax, qs, vs); break;
+            default: wilson_site<2, 3>(links, c, w0, rmax, tmax, qs, vs); break;
         }
     }
+    double v[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) v[k] = vs[k][threadIdx.x];
     block_sum16(v, partial + ((int64_t)blockIdx.x * 6 + plane) * 16);
 }
 
