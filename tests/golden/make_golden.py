@@ -1,8 +1,9 @@
 """Regenerate ``reference_vectors.json`` from the reference's own test vectors.
 
-Run in a container where the reference checkout is mounted at
-``/root/reference`` (read-only).  The GPU machines do not have that checkout,
-so the tests read only the JSON this script writes.  It copies, unchanged,
+Usage: ``python make_golden.py REFERENCE_ROOT`` (or set ``YM_REFERENCE_ROOT``),
+where REFERENCE_ROOT is a read-only checkout of the reference repository.
+Machines without that checkout run the tests from the JSON this script
+writes.  It copies, unchanged,
 the reference's ``test-vectors/*.json`` files that pin the hot path, plus the
 literal golden values the reference's Rust tests assert
 (``tests/su3_ensemble.rs``, ``tests/su2_ensemble.rs``,
@@ -12,7 +13,6 @@ import json
 import os
 import sys
 
-REFERENCE = os.environ.get("YM_REFERENCE_ROOT", "/root/reference")
 FILES = [
     "su2-ensemble-v1.json",
     "su2-observables-v1.json",
@@ -37,9 +37,13 @@ FILES = [
 
 
 def main() -> int:
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("YM_REFERENCE_ROOT")
+    if not root:
+        print("usage: make_golden.py REFERENCE_ROOT (or set YM_REFERENCE_ROOT)", file=sys.stderr)
+        return 2
     out = {"source": "QSOLKCB/YANG-MILLS test-vectors", "vectors": {}}
     for name in FILES:
-        with open(os.path.join(REFERENCE, "test-vectors", name)) as fh:
+        with open(os.path.join(root, "test-vectors", name)) as fh:
             out["vectors"][name] = json.load(fh)
     here = os.path.dirname(os.path.abspath(__file__))
     with open(os.path.join(here, "reference_vectors.json"), "w") as fh:
