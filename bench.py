@@ -50,6 +50,8 @@ ESS_CHAINS, ESS_EXTENTS = 16, [16, 16, 16, 16]
 ESS_SWEEPS = 3000                     # measured sweeps per sampler (one plaquette each)
 TRAIN_STEPS = 2000                    # configurations the plain sampler generates for training
 TRAIN_LR = 3e-3
+LOOP_BLOCKS = 10                      # loop measurements per run of the loop cadence
+LOOP_EVERY = 10                       # sweeps between Wilson / Polyakov measurements
 MASTER_SEED = 0x2C02198105010002
 LINK_BYTES = 144                      # FP64 3x3 complex
 LINKS_PER_UPDATE = 9                  # 8 link reads + 1 write per checkerboard update
@@ -66,6 +68,7 @@ def parse():
     ap.add_argument("--thermalization", type=int, default=THERMALIZATION)
     ap.add_argument("--ess-sweeps", type=int, default=ESS_SWEEPS)
     ap.add_argument("--train-steps", type=int, default=TRAIN_STEPS)
+    ap.add_argument("--loop-blocks", type=int, default=LOOP_BLOCKS)
     return ap.parse_args()
 
 
@@ -105,6 +108,8 @@ class ClockSampler:
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
+    INTERVAL_MS = 10
+
     def __init__(self, device: int):
         self.device = device
         self.proc = None
@@ -123,7 +128,7 @@ class ClockSampler:
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.fh,
+                 "--format=csv,noheader,nounits", "-lms", str(self.INTERVAL_MS)], stdout=self.fh,
                 stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -149,11 +154,13 @@ class ClockSampler:
                 self.proc.kill()
             self.fh.close()
 
-    def summary(self):
+    def summary(self, whole=False):
+        """Samples inside the timed region (whole: every sample the sampler
+        took, from before the warm-up steps to after the timed ones)."""
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         rows = [[p.strip() for p in ln.split(",")] for ln in self._rows()]
-        inside = rows[self.first:self.last]
+        inside = rows if whole else rows[self.first:self.last]
         if not inside:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"],
                     "samples": 0}
@@ -169,7 +176,19 @@ class ClockSampler:
         reasons = sorted({names[i] for r in inside for i in range(4) if r[5 + i] == "Active"})
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
-                "samples": len(inside), "interval_ms": 100}
+                "samples": len(inside), "interval_ms": self.INTERVAL_MS}
+
+
+def cpu_model():
+    """The host CPU's model name (/proc/cpuinfo)."""
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for ln in fh:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
 
 def cpu_baseline(seconds_target=12.0):
@@ -183,9 +202,13 @@ def cpu_baseline(seconds_target=12.0):
     per_thread = max(32, int(seconds_target * n / max(t, 1e-9)))
     secs, done = O.bench_su3_reference(ext, BETA, ANGLE, MASTER_SEED, threads, per_thread)
     return {"value": done / secs, "unit": UNIT, "cores": threads, "kind": "port",
+            "cpu_model": cpu_model(),
             "sample": f"{threads} threads x {per_thread} link visits (8 ordered hits each) of an "
                       f"independent cold 16^4 lattice, beta={BETA}, angle={ANGLE}, "
-                      f"{secs:.1f} s wall"}
+                      f"{secs:.1f} s wall; the lattices start cold (the reference's run_chain "
+                      "start), which does not change the cost of a visit: the reference's visit "
+                      "does the same twelve-plaquette products, exponential and checks whatever "
+                      "the link values"}
 
 
 def run_reference(args):
@@ -209,7 +232,9 @@ def run_reference(args):
         total_n += done
     value = total_n / total_s
     sample = (f"each step: {threads} threads x {per_thread} link visits of independent cold 16^4 "
-              f"lattices (reference algorithm restated in C, not the reference binary)")
+              f"lattices (reference algorithm restated in C, not the reference binary; a cold "
+              f"start does not change the cost of a visit, whose products and checks are the "
+              f"same whatever the link values)")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total_s / args.steps,
@@ -219,7 +244,7 @@ def run_reference(args):
                    "lattice": "16^4 per thread (reference cap 2^18 links)",
                    "parallelism": f"{threads} independent chains, one per host thread"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": sample},
+                         "cpu_model": cpu_model(), "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
 
@@ -250,7 +275,14 @@ def main():
     def timed_leg(ens, step, link_bytes, kernel, sampler_clocks=False):
         """W warm-up steps, then args.steps steps (step() = one sweep) each
         followed by the plaquette, timed with CUDA events on the handle's
-        stream; per-launch time of the dominant kernel from event pairs."""
+        stream; per-launch time of the dominant kernel from event pairs.
+        With sampler_clocks, nvidia-smi samples every 10 ms from before the
+        warm-up to after the timed steps: "clocks" summarises the samples
+        inside the timed region, "clocks_leg" all of them."""
+        sampler = ClockSampler(local) if sampler_clocks else None
+        if sampler:
+            sampler.__enter__()
+            sampler.wait_first()
         for _ in range(args.warmup):
             step()
             ens.average_plaquette()
@@ -262,9 +294,7 @@ def main():
         ens.profile(True)
         barrier()
         torch.cuda.synchronize()
-        sampler = ClockSampler(local) if sampler_clocks else None
         if sampler:
-            sampler.__enter__()
             sampler.wait_first()
         start.record(stream)
         for _ in range(args.steps):
@@ -292,6 +322,7 @@ def main():
                          "launch_ms": launch_s * 1e3, "kernel_share_of_step": k_ms / ms,
                          "bytes_per_launch": bytes_per_launch},
             "clocks": sampler.summary() if sampler else None,
+            "clocks_leg": sampler.summary(whole=True) if sampler else None,
         }
 
     # one thermalised 32^4 lattice (two-row binary32; wide-angle sweeps relax
@@ -394,6 +425,57 @@ def main():
         "peak_gbs": peak, "peak_source": f"{peak_kind} hbm_gbs",
         "note": "per call on the 32^4 FP64 lattice; achieved = compulsory bytes / CUDA-event time"}
 
+    # the loop-measurement cadence (two-row FP32 sweeps with FP64
+    # reunitarisation and plaquette every sweep; Wilson loops R x T <= 4 x 4
+    # and Polyakov loops every LOOP_EVERY sweeps, one captured graph per
+    # block) at 32^4 and 24^3 x 48, each against an FP64 run of the same
+    # length from the same field, seeds and sweep indices
+    from ymgpu.pipelines import fp32_vs_fp64_run
+
+    def loop_cadence(start):
+        c = fp32_vs_fp64_run(start, n_blocks=args.loop_blocks, sweeps_per_block=LOOP_EVERY,
+                             proposal_angle=ANGLE, generator_mode="ordered")
+        out = {}
+        for name, r in (("fp32_two_row", c.fp32), ("fp64", c.fp64)):
+            out[name] = {"link_updates_per_s": world * r.link_updates_per_s, "seconds": r.seconds,
+                         "sweep_only_seconds": r.sweep_seconds,
+                         "loop_measurement_seconds": r.loop_measurement_seconds,
+                         "loop_measurement_share": r.loop_measurement_seconds / r.seconds,
+                         "plaquette_mean": float(r.plaquette.mean()),
+                         "wilson_1x1_mean": float(r.wilson[:, :, :, 0, 0].mean()),
+                         "wilson_4x4_mean": float(r.wilson[:, :, :, 3, 3].mean()),
+                         "polyakov_abs_mean": float(np.abs(r.polyakov).mean())}
+        out["error_fp32_vs_fp64"] = {
+            "plaquette_mean_difference": c.plaquette_error,
+            "plaquette_combined_standard_error": c.plaquette_combined_sigma,
+            "plaquette_difference_in_sigma": c.plaquette_error / c.plaquette_combined_sigma,
+            "first_sweep_plaquette_difference": c.first_sweep_plaquette_error,
+            "wilson_max_abs_difference": c.wilson_max_error,
+            "polyakov_max_abs_difference": c.polyakov_max_error,
+            "note": "trajectories separate after a few sweeps (decisions near the threshold "
+                    "flip), so the run means are compared with their combined standard error "
+                    "(reference estimator on the per-sweep series); the first sweep, from the "
+                    "same field and streams, directly"}
+        out["schedule"] = (f"{args.loop_blocks} blocks x {LOOP_EVERY} sweeps, half width {ANGLE}, "
+                           "8 ordered hits; plaquette every sweep, loops every block")
+        return out
+
+    cad_start = ens.like()
+    ens.copy_to(cad_start)
+    cad_start.sweep_index = ens.sweep_index
+    loop_runs = {"32^4": loop_cadence(cad_start)}
+    cad_start.close()
+    e48 = ymgpu.Ensemble([[24, 24, 24, 48]], BETA, seed, precision=ymgpu.F32_TWO_ROW,
+                         lift_reference_caps=True, device=local)
+    e48.hot_start()
+    e48.metropolis_sweeps(THERMALIZATION_ANGLE, args.thermalization, "uniform")
+    s48 = e48.like(precision=ymgpu.F64)
+    e48.convert_to(s48)
+    s48.sweep_index = e48.sweep_index
+    e48.close()
+    loop_runs["24^3x48"] = loop_cadence(s48)
+    s48.close()
+
     # plaquette ESS/s of the three samplers at 16 x 16^4 from one equilibrated state
     def ess_leg(e, run):
         e.synchronize()
@@ -417,12 +499,21 @@ def main():
     e16.copy_to(e32p)
     e32w = e16.like()
     e16.copy_to(e32w)
+    # matched control: plain uniform-generator Metropolis at the constant half
+    # width the trained network settles at (its mean over the lattice's
+    # links), past the reference's cap of 1.0 behind the handle's explicit lift
+    s_bar = float(np.mean(s_half))
+    e32c = e16.like()
+    e16.copy_to(e32c)
+    e32c.lift_angle_cap(True)
     n = args.ess_sweeps
     ess_f64 = ess_leg(e64, lambda: e64.measured_sweeps(ANGLE, n, 1, "ordered"))
     ess_f32 = ess_leg(e32p, lambda: e32p.measured_sweeps(ANGLE, n, 1, "uniform"))
     ess_f32w = ess_leg(e32w, lambda: e32w.measured_sweeps(1.0, n, 1, "uniform"))
+    ess_f32c = ess_leg(e32c, lambda: e32c.measured_sweeps(s_bar, n, 1, "uniform"))
+    ess_f32c["half_width"] = s_bar
     ess_lrn = ess_leg(e16, lambda: model.measured_sweeps(e16, n))
-    for e in (e64, e32p, e32w, e16):
+    for e in (e64, e32p, e32w, e32c, e16):
         e.close()
     model.close()
     sig = lambda a, b: abs(a["plaquette_mean"] - b["plaquette_mean"]) / np.hypot(
@@ -577,6 +668,8 @@ def main():
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": int(args.steps * 11),
             "clocks": leg["clocks"],
+            "clocks_leg": dict(leg["clocks_leg"] or {}, note="every sample of the FP64 leg: "
+                               "warm-up, timed steps and the sampler's start and stop"),
             "fp32_two_row": {
                 "value": f32["value"], "unit": UNIT, "dtype": "f32 links, f64 dS/accept/plaquette",
                 "ms_per_step": f32["ms"] / args.steps,
@@ -599,14 +692,23 @@ def main():
             "other_configs": configs_extra,
             "stout_32x4_fp64": stout,
             "observables_32x4_fp64": observables,
+            "loop_cadence_fp32_vs_fp64": loop_runs,
             "ess": {
                 "geometry": f"{ESS_CHAINS} chains x 16^4 (total volume of 32^4), beta=6.0, "
                             f"{n} measured sweeps per sampler from one equilibrated state",
                 "estimator": "reference diagnostics (initial positive window), per chain, summed",
                 "plain_f64_ordered_0.3": ess_f64, "plain_f32_uniform_0.3": ess_f32,
                 "plain_f32_uniform_1.0": ess_f32w, "learned_f32": ess_lrn,
+                "plain_f32_uniform_at_learned_scale": ess_f32c,
                 "control_note": "plain_f32_uniform_1.0 is plain Metropolis at the widest half "
-                                "width the reference admits",
+                                "width the reference admits; plain_f32_uniform_at_learned_scale "
+                                "is plain Metropolis with uniform generators at the constant "
+                                "half width the trained network settles at (the matched "
+                                "control: same scale, no per-link network)",
+                "learned_vs_constant_scale": ess_lrn["plaquette_ess_per_s"] /
+                                             ess_f32c["plaquette_ess_per_s"],
+                "tau_learned_vs_constant_scale": ess_lrn["tau_int"] / ess_f32c["tau_int"],
+                "plaquette_sigma_learned_vs_constant_scale": float(sig(ess_lrn, ess_f32c)),
                 "learned_vs_plain_f32_at_1.0": ess_lrn["plaquette_ess_per_s"] /
                                                ess_f32w["plaquette_ess_per_s"],
                 "learned_vs_plain_f64": ess_lrn["plaquette_ess_per_s"] / ess_f64["plaquette_ess_per_s"],

@@ -111,6 +111,30 @@ int32_t ym_su3_metropolis_sweeps(ym_ensemble *ens, double proposal_angle, int32_
 int32_t ym_su3_measured_sweeps(ym_ensemble *ens, double proposal_angle, int32_t generator_mode,
                                int64_t n_measurements, int64_t sweeps_per_measurement,
                                double *series);
+/* The run_chain cadence with loop observables (su3_ensemble.rs:408-480 for
+ * the sweep/measure order; the loops are path_holonomy.rs:172-260 and
+ * su3_lattice.rs:185-212 averaged over the lattice): n_blocks times
+ *   { sweeps_per_block x (one sweep, the average plaquette of every chain),
+ *     Wilson loops R x T <= rmax x tmax of every chain (ym_su3_wilson_loops),
+ *     Polyakov loops along polyakov_direction (ym_su3_polyakov_loops) },
+ * each block replayed from one captured CUDA graph with no host round trip.
+ * A two-row binary32 handle sweeps with binary64 reunitarisation after every
+ * sweep and an FP64 plaquette; its loops are measured on `view`, a binary64
+ * handle of the same extents that receives the converted links every block
+ * (for a binary64 handle `view` is NULL or the handle itself).
+ *   plaquette [n_blocks * sweeps_per_block][n_chains]
+ *   wilson    [n_blocks][n_chains][96] (layout of ym_su3_wilson_loops)
+ *   polyakov  [n_blocks][n_chains][2]  (mean re, im) */
+typedef struct {
+    double proposal_angle;
+    int32_t generator_mode;        /* YM_GEN_* */
+    int32_t polyakov_direction;    /* 0..3 */
+    int64_t n_blocks;              /* loop measurements */
+    int64_t sweeps_per_block;      /* sweeps between loop measurements, >= 1 */
+    int32_t rmax, tmax;            /* 1..4 */
+} ym_measured_run;
+int32_t ym_su3_measured_run(ym_ensemble *ens, ym_ensemble *view, const ym_measured_run *run,
+                            double *plaquette, double *wilson, double *polyakov);
 /* Sweep path of SU(3) FP64 handles (no reference counterpart).  When every
  * chain is small enough for its links to sit in one CTA's shared memory
  * (4^4 and similar), sweeps can run chain-resident: one launch does many
@@ -124,6 +148,15 @@ enum { YM_PATH_AUTO = -1, YM_PATH_TILED = 0, YM_PATH_RESIDENT = 1 };
 int32_t ym_ensemble_set_sweep_path(ym_ensemble *ens, int32_t path);
 /* The path in use: YM_PATH_AUTO while not yet decided. */
 int32_t ym_ensemble_get_sweep_path(ym_ensemble *ens, int32_t *path);
+
+/* Proposal half widths above the reference's cap of 1.0 (no reference
+ * counterpart: su3_ensemble.rs:28 rejects them).  With lift != 0 the sweeps
+ * of a two-row binary32 handle accept half widths up to 2.5, the range of
+ * the learned proposal's scale, so that plain Metropolis can run at the
+ * scale the learned proposal settles at (a matched control).  binary64
+ * handles keep the reference's cap: their exact exponential assumes
+ * |theta/2| < 1/2 (YM_ERR_UNSUPPORTED_PRECISION). */
+int32_t ym_ensemble_lift_angle_cap(ym_ensemble *ens, int32_t lift);
 
 /* Accumulated proposals/accepts per chain since creation or reset
  * (MetropolisAccounting su3_ensemble.rs:117-121). */
@@ -178,9 +211,10 @@ int32_t ym_average_plaquette(ym_ensemble *ens, double *per_chain);
  *   links   device pointer, 16-byte aligned, to one SU(3) lattice in the
  *           reference layout (link = site*4+mu, 18 doubles each);
  *   extents host array of 4 extents, each >= 2;
- *   out     device pointer receiving one double, the same mean the
- *           allocating entry point returns (it is not checked for
- *           finiteness);
+ *   out     device pointer receiving one double, the average plaquette:
+ *           within 1e-12 relative of ym_average_plaquette's value (the two
+ *           sum in different orders, so they need not agree bit for bit;
+ *           it is not checked for finiteness);
  *   stream  cudaStream_t to enqueue on (NULL: the legacy default stream).
  * Asynchronous: the value is in `out` once the stream reaches it.  Scratch
  * is a file-scope device array of 65536 doubles (512 KiB) that every GPU
@@ -188,8 +222,10 @@ int32_t ym_average_plaquette(ym_ensemble *ens, double *per_chain);
  * fail with YM_ERR_SCRATCH_TOO_SMALL before any device work.  All calls
  * share that array: calls that overlap on the GPU (concurrent streams or
  * threads) race and must be serialised by the caller.  The first call on a
- * device resolves the array's device address for that device; make that
- * first call before any stream capture. */
+ * device resolves the array's device address for that device (and the first
+ * call after a device reset resolves it again); make that first call before
+ * any stream capture.  A CUDA failure returns YM_ERR_CUDA with the error
+ * readable through ym_last_cuda_error. */
 int32_t ym_su3_average_plaquette_noalloc(const double *links, const int64_t *extents,
                                          double *out, void *stream);
 
@@ -206,6 +242,92 @@ int32_t ym_su3_wilson_loops(ym_ensemble *ens, int32_t rmax, int32_t tmax, double
 /* Polyakov loop (su3_lattice.rs:185-212) averaged over every start site with
  * x_dir = 0: out[chain*2 + 0] = mean Re, out[chain*2 + 1] = mean Im. */
 int32_t ym_su3_polyakov_loops(ym_ensemble *ens, int32_t direction, double *out);
+/* SU(2) lattice averages of the reference's loops: for every chain, plane
+ * and R <= rmax, T <= tmax (1..4) the mean over start sites of
+ * Lattice4::rectangular_wilson_loop(x, mu, nu, R, T) (lib.rs:471-481, the
+ * single left-to-right product of rectangular_path's steps, half real
+ * trace), laid out as ym_su3_wilson_loops; and the mean over the lines along
+ * `direction` of Lattice4::polyakov_loop (lib.rs:483-505), one double per
+ * chain.  The lattice averages have no reference counterpart; each per-site
+ * value is the reference's primitive with its arithmetic. */
+int32_t ym_su2_wilson_loops(ym_ensemble *ens, int32_t rmax, int32_t tmax, double *out);
+int32_t ym_su2_polyakov_loops(ym_ensemble *ens, int32_t direction, double *out);
+
+/* ---- per-site and per-link queries (Su3Lattice4, Lattice4, path_holonomy)
+ * on binary64 handles of either group.  Sites are given as 4 coordinates
+ * (x0, x1, x2, x3) and per-site outputs are in the reference's lexicographic
+ * site order (x3 fastest).  A path is a list of steps: +(d+1) steps forward
+ * along direction d, -(d+1) backward (path_holonomy::OrientedStep,
+ * lib.rs PathStep).  SU(3) products are the reference's checked products
+ * (Su3::mul su3.rs:286-288): a product outside the 5e-12 group gates fails
+ * with YM_ERR_NON_FINITE_MATRIX / YM_ERR_NON_UNITARY_MATRIX /
+ * YM_ERR_DETERMINANT_NOT_ONE.  Every value below is bit for bit the
+ * reference's arithmetic in the reference's order. ---- */
+
+/* path_holonomy::rectangular_path (path_holonomy.rs:219-260; lib.rs:438-469):
+ * R steps forward along mu, T forward along nu, R back, T back.  steps has
+ * room for `capacity` entries; *n_steps = 2(R+T). */
+int32_t ym_rectangular_path(int32_t mu, int32_t nu, int64_t r, int64_t t, int32_t *steps,
+                            int64_t capacity, int64_t *n_steps);
+/* path_holonomy (path_holonomy.rs:132-161; Lattice4::path_holonomy
+ * lib.rs:384-414): the ordered product along `steps` from `start` (18 doubles
+ * SU(3), 4 doubles SU(2)); end (optional) receives the final site. */
+int32_t ym_path_holonomy(ym_ensemble *ens, int64_t chain, const int64_t *start,
+                         const int32_t *steps, int64_t n_steps, double *holonomy, int64_t *end);
+/* wilson_loop (path_holonomy.rs:172-181: (1/3) Tr of the closed holonomy,
+ * complex; Lattice4::wilson_loop lib.rs:430-436: (1/2) Re Tr, imaginary part
+ * 0) at one start (out2 = re, im) or from every site of the chain
+ * (out[2*lex], out[2*lex+1]).  An open path fails with
+ * YM_ERR_PATH_NOT_CLOSED. */
+int32_t ym_wilson_loop(ym_ensemble *ens, int64_t chain, const int64_t *start, const int32_t *steps,
+                       int64_t n_steps, double *out2);
+int32_t ym_wilson_loop_sites(ym_ensemble *ens, int64_t chain, const int32_t *steps, int64_t n_steps,
+                             double *out);
+/* Su3Lattice4::polyakov_loop(start, direction) (su3_lattice.rs:185-212,
+ * complex (1/3) Tr) / Lattice4::polyakov_loop (lib.rs:483-505, (1/2) Re Tr,
+ * imaginary part 0) at one start or from every site. */
+int32_t ym_polyakov_loop(ym_ensemble *ens, int64_t chain, const int64_t *start, int32_t direction,
+                         double *out2);
+int32_t ym_polyakov_loop_sites(ym_ensemble *ens, int64_t chain, int32_t direction, double *out);
+/* plaquette(x, mu, nu) (su3_lattice.rs:168-181: the SU(3) matrix, 18
+ * doubles; lib.rs:348-361: the SU(2) quaternion, 4 doubles). */
+int32_t ym_plaquette(ym_ensemble *ens, int64_t chain, const int64_t *x, int32_t mu, int32_t nu,
+                     double *out);
+/* wilson_action(beta) per chain (su3_lattice.rs:214-242: beta * sum of
+ * 1 - (1/3) Re Tr P; lib.rs:363-382: beta * sum of 1 - (1/2) Re Tr P), the
+ * terms summed in the reference's sequential order. */
+int32_t ym_wilson_action(ym_ensemble *ens, double beta, double *per_chain);
+/* Lattice4::staple (lib.rs:507-546): the unnormalised sum of the six staple
+ * products of link (x, mu), 4 components; *terms = 6. */
+int32_t ym_su2_staple(ym_ensemble *ens, int64_t chain, const int64_t *x, int32_t mu, double *comp4,
+                      int64_t *terms);
+/* local_link_action (su3_ensemble.rs:311-317) and local_action_difference
+ * (su3_ensemble.rs:319-334) of link (x, mu): beta times the sum over the six
+ * forward and six backward plaquettes holding the link of
+ * 1 - (1/3) Re Tr P; the difference between the candidate (18 doubles) and
+ * the stored link.  beta in [0, 12]. */
+int32_t ym_su3_local_link_action(ym_ensemble *ens, int64_t chain, const int64_t *x, int32_t mu,
+                                 double beta, double *out);
+int32_t ym_su3_local_action_difference(ym_ensemble *ens, int64_t chain, const int64_t *x,
+                                       int32_t mu, const double *candidate, double beta,
+                                       double *out);
+/* Su3Lattice4::gauge_transform (su3_lattice.rs:244-283): chain dst_chain of
+ * dst (same extents; dst may be src) receives g(x) U_mu(x) g(x+mu)^dag for
+ * every link of chain `chain` of src, each product checked.  site_gauges is a
+ * host array of V SU(3) matrices (18 doubles each) in lexicographic site
+ * order: the reference's closure evaluated at every site. */
+int32_t ym_su3_gauge_transform(ym_ensemble *src, int64_t chain, const double *site_gauges,
+                               ym_ensemble *dst, int64_t dst_chain);
+/* Su3Lattice4::link / set_link (su3_lattice.rs:153-166), Lattice4::link /
+ * set_link: one link (18 doubles SU(3), 4 SU(2)) moved between the host and
+ * the device without touching the rest of the chain.  On two-row binary32
+ * handles link() returns the binary64 image (third row rebuilt) and
+ * set_link() stores the first two rows rounded to binary32. */
+int32_t ym_ensemble_get_link(ym_ensemble *ens, int64_t chain, const int64_t *x, int32_t mu,
+                             double *out);
+int32_t ym_ensemble_set_link(ym_ensemble *ens, int64_t chain, const int64_t *x, int32_t mu,
+                             const double *value);
+
 /* scalar_a1pp_operator_basis (glueball_operators.rs:93-160) for every time
  * slice of every chain: the mean of Re W over the three 1x1 and the six 2x1
  * spatial orientations and all spatial start sites.  Outputs packed chain by

@@ -284,6 +284,24 @@ def su3_polyakov_loop(extents, links, start, direction) -> complex:
     return complex(re.value, im.value)
 
 
+def su3_plaquette_matrix(extents, links, x, mu, nu) -> np.ndarray:
+    out = np.zeros((3, 3), np.complex128)
+    _check(lib().or_su3_plaquette_matrix(_ext(extents), _dp(links.view(np.float64)), _x(x), mu,
+                                         nu, _dp(out.view(np.float64))), "plaquette_matrix")
+    return out
+
+
+def su3_path_holonomy(extents, links, start, steps):
+    s = np.ascontiguousarray(steps, np.int32)
+    out = np.zeros((3, 3), np.complex128)
+    end = np.zeros(4, np.int64)
+    _check(lib().or_su3_path_holonomy(_ext(extents), _dp(links.view(np.float64)), _x(start),
+                                      s.ctypes.data_as(P(C.c_int32)), len(s),
+                                      _dp(out.view(np.float64)),
+                                      end.ctypes.data_as(P(i64))), "path_holonomy")
+    return out, tuple(int(v) for v in end)
+
+
 def rectangular_path(mu, nu, r, t) -> np.ndarray:
     steps = np.zeros(2 * (r + t) + 8, np.int32)
     n = i64()
@@ -401,6 +419,13 @@ def su2_polyakov_loop(extents, links, start, direction) -> float:
     _check(lib().or_su2_polyakov_loop(_ext(extents), _dp(links), _x(start), direction,
                                       C.byref(out)), "su2 polyakov")
     return out.value
+
+
+def su2_plaquette(extents, links, x, mu, nu) -> np.ndarray:
+    out = np.zeros(4, np.float64)
+    _check(lib().or_su2_plaquette(_ext(extents), _dp(links), _x(x), mu, nu, _dp(out)),
+           "su2 plaquette")
+    return out
 
 
 def su2_staple(extents, links, x, mu) -> np.ndarray:

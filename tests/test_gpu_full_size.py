@@ -8,8 +8,9 @@ the oracle to sweep the whole lattice.
   later ones at their pre-sweep values — and must equal the GPU's links bit
   for bit; the lattice plaquette matches the oracle's sequential sum to
   1e-12 relative and the links stay in SU(3) to 1e-12.
-* 32^4 two-row FP32: one sweep from the same field, seed and sweep index as
-  the FP64 sweep stays within the FP32 path's stated error of it.
+* 32^4 and 24^3 x 48 two-row FP32: one sweep from the same field, seed and
+  sweep index as the FP64 sweep stays within the FP32 path's stated error of
+  it.
 * SU(2) 10^4 at beta 2.3 (the heat-bath workload): the GPU sweep equals the
   oracle's checkerboard sweep (overrelaxation bitwise, heat-bath to 1e-12).
 * 64 chains of 4^4 (the batched-chain workload): chains across the batch
@@ -105,13 +106,14 @@ def test_full_size_sweep_sampled_links_bitwise(oracle, ext, uniform):
     assert ures[0] <= 1e-12 and dres[0] <= 1e-12
 
 
-def test_full_size_fp32_sweep_error_against_fp64(oracle):
-    """The two-row binary32 sweep at 32^4, from the same field, seed and sweep
-    index as the FP64 sweep (bitwise the oracle's, above): >= 98% of links
-    within 1e-5 of the FP64 result (a decision may flip where the uniform
-    lies within the ~1e-6 dS error of exp(-dS)), plaquettes within 1e-6."""
+@pytest.mark.parametrize("ext", [[32, 32, 32, 32], [24, 24, 24, 48]])
+def test_full_size_fp32_sweep_error_against_fp64(oracle, ext):
+    """The two-row binary32 sweep at 32^4 and 24^3 x 48, from the same field,
+    seed and sweep index as the FP64 sweep (bitwise the oracle's, above):
+    >= 98% of links within 1e-5 of the FP64 result (a decision may flip where
+    the uniform lies within the ~1e-6 dS error of exp(-dS)), plaquettes
+    within 1e-6."""
     import ymgpu
-    ext = [32, 32, 32, 32]
     seed = oracle.derive_su3_chain_seed(MASTER, 5)
     with ymgpu.Ensemble([ext], 6.0, seed, lift_reference_caps=True) as e64, \
             ymgpu.Ensemble([ext], 6.0, seed, precision=ymgpu.F32_TWO_ROW,

@@ -133,10 +133,18 @@ def test_training_raises_objective():
     assert s.mean() > 0.45           # started at 0.3
 
 
-def test_trained_proposal_beats_plain():
-    """Plaquette autocorrelation per sweep: the trained proposal against
-    plain Metropolis with uniform generators at half width 0.3, same
-    lattices, same plaquette within errors."""
+def test_trained_proposal_against_constant_scale_control():
+    """What the trained network gains, judged by plaquette autocorrelation
+    per sweep against two plain Metropolis controls with uniform
+    generators, same lattices, plaquettes equal within errors:
+
+    * the matched control, at the constant half width the network itself
+      settles at (its mean over the links; past the reference's cap of 1.0,
+      behind the handle's explicit lift): the network must do as well as
+      that tuned constant (tau within 20%) -- its gain is finding the scale
+      by training, the per-link spread of its output adds nothing measurable;
+    * the reference's half width 0.3: both the network and the matched
+      control must shorten tau by at least 1.5x."""
     import ymgpu
     from ymgpu.su2_ensemble import diagnostics
     nch, meas = 32, 1500
@@ -145,21 +153,31 @@ def test_trained_proposal_beats_plain():
         hist = model.train(ens, 2000, sweeps_per_step=1, plain_angle=0.3, lr=3e-3)
         f, _, _ = ymgpu.learned.records(ens, 0, 0)
         p_gen, s_half = ymgpu.learned.proposal(model.forward(f))
+        s_bar = float(s_half.mean())
         plain = ens.like()
         ens.copy_to(plain)
+        matched = ens.like()
+        ens.copy_to(matched)
+        matched.lift_angle_cap(True)
         model.sweeps(ens, 200)
         plain.metropolis_sweeps(0.3, 200, "uniform")
+        matched.metropolis_sweeps(s_bar, 200, "uniform")
         s_l = model.measured_sweeps(ens, meas)
         s_p = plain.measured_sweeps(0.3, meas, 1, "uniform")
+        s_c = matched.measured_sweeps(s_bar, meas, 1, "uniform")
         plain.close()
+        matched.close()
     tau = lambda s: np.mean([diagnostics(s[:, c], 200)[0].integrated_autocorrelation_time
                              for c in range(nch)])
-    t_l, t_p = tau(s_l), tau(s_p)
-    m_l, m_p = s_l.mean(0), s_p.mean(0)
-    err = np.hypot(m_l.std(ddof=1), m_p.std(ddof=1)) / np.sqrt(nch)
-    assert abs(m_l.mean() - m_p.mean()) <= 4 * err, (m_l.mean(), m_p.mean(), err)
-    info = (t_l, t_p, s_half.mean(), p_gen.mean(0), hist[:3], hist[-3:])
-    assert t_l < t_p / 1.5, info
+    t_l, t_p, t_c = tau(s_l), tau(s_p), tau(s_c)
+    for other in (s_p, s_c):
+        m_l, m_o = s_l.mean(0), other.mean(0)
+        err = np.hypot(m_l.std(ddof=1), m_o.std(ddof=1)) / np.sqrt(nch)
+        assert abs(m_l.mean() - m_o.mean()) <= 4 * err, (m_l.mean(), m_o.mean(), err)
+    info = (t_l, t_c, t_p, s_bar, p_gen.mean(0), hist[:3], hist[-3:])
+    assert 1.0 < s_bar < 2.5, info
+    assert t_l <= 1.2 * t_c, info
+    assert t_l < t_p / 1.5 and t_c < t_p / 1.5, info
 
 
 def test_bounded_wait_gives_up_and_device_stays_usable():

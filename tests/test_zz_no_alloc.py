@@ -5,9 +5,11 @@ pool owns the GPU and only lends out buffers it allocated, or a deployment
 that must keep a fixed device footprint after start-up.  Called through the
 C ABI with device buffers the test allocates (the entry point allocates
 nothing), its result must equal the allocating entry point's
-(ym_average_plaquette) within the plaquette tolerance of the other tests,
-1e-12 relative, on two calls in a row.  This file is collected last so a run
-that stops at the first failure has already run every other test.
+(ym_average_plaquette) and the oracle's sequential sum within the plaquette
+tolerance of the other tests, 1e-12 relative, on two calls in a row, and the
+device's free memory must not move across a call.  This file is collected
+last so a run that stops at the first failure has already run every other
+test.
 """
 import ctypes as C
 
@@ -53,7 +55,31 @@ def test_noalloc_plaquette_equals_allocating_entry_point(oracle):
     got2 = _noalloc(torch, ext, second)       # second call in a row reuses the scratch
     assert abs(got1 - ref1) <= 1e-12 * abs(ref1)
     assert abs(got2 - ref2) <= 1e-12 * abs(ref2)
+    for got, links in ((got1, first), (got2, second)):
+        want = oracle.su3_average_plaquette(ext, links)
+        assert abs(got - want) <= 1e-12 * abs(want)
     assert got1 != got2
+
+
+def test_noalloc_plaquette_takes_no_device_memory(oracle):
+    torch = pytest.importorskip("torch")
+    import ymgpu
+    ext = [8, 8, 8, 6]
+    links = _rough(oracle, ext, 5)
+    d_links = torch.from_numpy(links.view(np.float64).reshape(-1).copy()).cuda()
+    d_out = torch.zeros(1, dtype=torch.float64, device="cuda")
+    e = (C.c_int64 * 4)(*ext)
+    fn = ymgpu.lib().ym_su3_average_plaquette_noalloc
+    assert fn(C.c_void_p(d_links.data_ptr()), e, C.c_void_p(d_out.data_ptr()), None) == 0
+    torch.cuda.synchronize()
+    free_before, _ = torch.cuda.mem_get_info()
+    for _ in range(3):
+        assert fn(C.c_void_p(d_links.data_ptr()), e, C.c_void_p(d_out.data_ptr()), None) == 0
+    torch.cuda.synchronize()
+    free_after, _ = torch.cuda.mem_get_info()
+    assert free_after == free_before
+    want = oracle.su3_average_plaquette(ext, links)
+    assert abs(float(d_out.item()) - want) <= 1e-12 * abs(want)
 
 
 def test_noalloc_rejects_lattices_beyond_its_scratch():

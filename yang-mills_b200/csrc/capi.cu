@@ -27,6 +27,12 @@ int32_t cuda_status(cudaError_t err) {
     return YM_ERR_CUDA;
 }
 
+}  // namespace
+
+int32_t ym::record_cuda_status(cudaError_t err) { return cuda_status(err); }
+
+namespace {
+
 #define YM_CUDA(call)                                 \
     do {                                              \
         cudaError_t err__ = (call);                   \
@@ -39,6 +45,7 @@ constexpr double kMaxSu3Beta = 12.0;                 // su3_ensemble.rs:24
 constexpr double kMaxSu2Beta = 8.0;                  // su2_ensemble.rs:18
 constexpr double kMinAngle = 1.0e-8;                 // su3_ensemble.rs:27
 constexpr double kMaxAngle = 1.0;                    // su3_ensemble.rs:28
+constexpr double kLiftedMaxAngle = 2.5;              // two-row sweeps with the cap lifted
 constexpr int kGraphSweeps = 8;                      // sweeps per captured graph
 
 template <class T>
@@ -49,7 +56,11 @@ cudaError_t dalloc(T **p, size_t count) {
 void free_all(ym_ensemble *e) {
     if (e->sweep_graph) cudaGraphExecDestroy(e->sweep_graph);
     if (e->measure_graph) cudaGraphExecDestroy(e->measure_graph);
+    if (e->run_graph) cudaGraphExecDestroy(e->run_graph);
     if (e->d_series) cudaFree(e->d_series);
+    if (e->d_wilson_series) cudaFree(e->d_wilson_series);
+    if (e->d_poly_series) cudaFree(e->d_poly_series);
+    if (e->d_loop_row) cudaFree(e->d_loop_row);
     if (e->d_series_row) cudaFree(e->d_series_row);
     for (auto &pool : e->events)
         for (auto &p : pool) {
@@ -61,7 +72,7 @@ void free_all(ym_ensemble *e) {
                     e->d_result2, e->d_accepts, e->d_sweep, e->d_rng, e->d_ref_counts,
                     e->d_error, e->d_obs_partial, e->d_obs_out, e->d_site_vals,
                     e->d_slice_chain, e->d_slice_t, e->d_slice_plaq, e->d_slice_rect,
-                    e->d_links_tmp};
+                    e->d_links_tmp, e->d_query_error, e->d_query, e->d_steps, e->d_terms};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (e->stream) cudaStreamDestroy(e->stream);
@@ -71,6 +82,15 @@ int32_t validate_angle(double a) {
     if (!std::isfinite(a) || a < kMinAngle || a > kMaxAngle)
         return YM_ERR_PROPOSAL_ANGLE_OUTSIDE_REFERENCE_RANGE;
     return YM_OK;
+}
+
+// The half width a handle's sweeps accept: the reference's [1e-8, 1], or up
+// to kLiftedMaxAngle on a two-row handle whose angle cap was lifted.
+int32_t validate_angle_for(const ym_ensemble *e, double a) {
+    if (e->angle_cap_lifted && e->precision == YM_PREC_F32_TWO_ROW &&
+        std::isfinite(a) && a > kMaxAngle && a <= kLiftedMaxAngle)
+        return YM_OK;
+    return validate_angle(a);
 }
 
 int32_t validate_su3_betas(const ym_ensemble *e) {
@@ -469,7 +489,7 @@ int32_t ym_su3_metropolis_sweeps(ym_ensemble *e, double angle, int32_t generator
     // metropolis_sweep validates beta before the angle (su3_ensemble.rs:348-351)
     int32_t st = validate_su3_betas(e);
     if (st) return st;
-    st = validate_angle(angle);
+    st = validate_angle_for(e, angle);
     if (st) return st;
     if (generator_mode != YM_GEN_ORDERED && generator_mode != YM_GEN_UNIFORM) return YM_ERR_INVALID_ARGUMENT;
     if (n_sweeps < 0) return YM_ERR_INVALID_ARGUMENT;
@@ -551,10 +571,16 @@ int32_t ym_su3_metropolis_sweeps(ym_ensemble *e, double angle, int32_t generator
 // row counter.  The captured measurement graph stores into d_series by
 // address, so growing the buffer also drops that graph: a graph replayed
 // after the reallocation would write into the freed buffer.
+static void drop_run_graph(ym_ensemble *e) {
+    if (e->run_graph) cudaGraphExecDestroy(e->run_graph);
+    e->run_graph = nullptr;
+}
+
 static cudaError_t ensure_series(ym_ensemble *e, int64_t n_measurements) {
     if (e->series_capacity < n_measurements) {
         if (e->measure_graph) cudaGraphExecDestroy(e->measure_graph);
         e->measure_graph = nullptr;
+        drop_run_graph(e);
         if (e->d_series) cudaFree(e->d_series);
         e->d_series = nullptr;
         e->series_capacity = 0;
@@ -575,7 +601,7 @@ int32_t ym_su3_measured_sweeps(ym_ensemble *e, double angle, int32_t generator_m
     if (e->group != YM_GROUP_SU3) return YM_ERR_WRONG_GROUP;
     int32_t st = validate_su3_betas(e);
     if (st) return st;
-    st = validate_angle(angle);
+    st = validate_angle_for(e, angle);
     if (st) return st;
     if (generator_mode != YM_GEN_ORDERED && generator_mode != YM_GEN_UNIFORM) return YM_ERR_INVALID_ARGUMENT;
     if (n_measurements < 0 || sweeps_per_measurement < 0) return YM_ERR_INVALID_ARGUMENT;
@@ -651,6 +677,142 @@ int32_t ym_su3_measured_sweeps(ym_ensemble *e, double angle, int32_t generator_m
     for (int64_t ch = 0; ch < e->n_chains; ++ch)
         e->proposals[ch] += (uint64_t)(n_measurements * sweeps_per_measurement) * 32u *
                             (uint64_t)e->chains[ch].volume;
+    return YM_OK;
+}
+
+static cudaError_t ensure_loop_series(ym_ensemble *e, int64_t rows) {
+    if (e->loop_capacity < rows) {
+        drop_run_graph(e);
+        if (e->d_wilson_series) cudaFree(e->d_wilson_series);
+        if (e->d_poly_series) cudaFree(e->d_poly_series);
+        e->d_wilson_series = nullptr;
+        e->d_poly_series = nullptr;
+        e->loop_capacity = 0;
+        cudaError_t err = dalloc(&e->d_wilson_series, (size_t)(rows * e->n_chains * 96));
+        if (err == cudaSuccess) err = dalloc(&e->d_poly_series, (size_t)(rows * e->n_chains * 2));
+        if (err != cudaSuccess) return err;
+        e->loop_capacity = rows;
+    }
+    if (!e->d_loop_row) return dalloc(&e->d_loop_row, 1);
+    return cudaSuccess;
+}
+
+int32_t ym_su3_measured_run(ym_ensemble *e, ym_ensemble *view, const ym_measured_run *run,
+                            double *plaquette, double *wilson, double *polyakov) {
+    if (!e || !run) return YM_ERR_NULL_ARGUMENT;
+    if (run->n_blocks > 0 && (!plaquette || !wilson || !polyakov)) return YM_ERR_NULL_ARGUMENT;
+    if (e->group != YM_GROUP_SU3) return YM_ERR_WRONG_GROUP;
+    int32_t st = validate_su3_betas(e);
+    if (st) return st;
+    if ((st = validate_angle_for(e, run->proposal_angle))) return st;
+    const int32_t mode = run->generator_mode;
+    if (mode != YM_GEN_ORDERED && mode != YM_GEN_UNIFORM) return YM_ERR_INVALID_ARGUMENT;
+    if (run->n_blocks < 0 || run->sweeps_per_block < 1) return YM_ERR_INVALID_ARGUMENT;
+    if (run->rmax == 0 || run->tmax == 0) return YM_ERR_ZERO_RECTANGLE_EXTENT;
+    if (run->rmax < 0 || run->tmax < 0 || run->rmax > 4 || run->tmax > 4) return YM_ERR_INVALID_ARGUMENT;
+    if (run->polyakov_direction < 0 || run->polyakov_direction >= 4) return YM_ERR_DIRECTION_OUT_OF_RANGE;
+    if ((st = require_checkerboard(e))) return st;
+    // The loops read binary64 links: a two-row handle is measured through a
+    // binary64 handle of the same extents that receives its converted image.
+    ym_ensemble *m = e;
+    if (f32(e)) {
+        if (!view) return YM_ERR_NULL_ARGUMENT;
+        if (view->group != YM_GROUP_SU3) return YM_ERR_WRONG_GROUP;
+        if (view->precision != YM_PREC_F64) return YM_ERR_UNSUPPORTED_PRECISION;
+        if (view->n_chains != e->n_chains || view->device != e->device) return YM_ERR_LATTICE_EXTENTS_MISMATCH;
+        for (int64_t ch = 0; ch < e->n_chains; ++ch)
+            for (int d = 0; d < 4; ++d)
+                if (view->chains[ch].n[d] != e->chains[ch].n[d]) return YM_ERR_LATTICE_EXTENTS_MISMATCH;
+        m = view;
+    } else if (view && view != e) {
+        return YM_ERR_INVALID_ARGUMENT;
+    }
+    if ((st = set_device(e))) return st;
+    if (run->n_blocks == 0) return YM_OK;
+    const int64_t spb = run->sweeps_per_block, rows = run->n_blocks * spb;
+    YM_CUDA(ensure_obs_scratch(m));
+    if (m != e) YM_CUDA(cudaStreamSynchronize(m->stream));   // m's earlier work is done
+    YM_CUDA(ensure_series(e, rows));
+    YM_CUDA(ensure_loop_series(e, run->n_blocks));
+    YM_CUDA(cudaMemsetAsync(e->d_series_row, 0, sizeof(uint64_t), e->stream));
+    YM_CUDA(cudaMemsetAsync(e->d_loop_row, 0, sizeof(uint64_t), e->stream));
+    const double angle = run->proposal_angle;
+    auto block = [&]() -> cudaError_t {
+        for (int64_t k = 0; k < spb; ++k) {
+            for (int parity = 0; parity < 2; ++parity)
+                for (int mu = 0; mu < 4; ++mu) {
+                    cudaError_t err = f32(e) ? ym::launch_f32_metropolis(e, parity, mu, angle, mode)
+                                             : ym::launch_su3_metropolis(e, parity, mu, angle, mode);
+                    if (err != cudaSuccess) return err;
+                }
+            cudaError_t err = f32(e) ? ym::launch_f32_reunitarize(e) : cudaSuccess;
+            if (err == cudaSuccess) err = ym::launch_advance_sweep(e);
+            if (err == cudaSuccess) err = f32(e) ? ym::launch_f32_plaquette_partials(e) : ym::launch_su3_plaquette(e);
+            if (err == cudaSuccess && f32(e)) err = ym::launch_chain_reduce(e, e->d_partial, e->d_result, 0, 6.0);
+            if (err == cudaSuccess) err = ym::launch_store_series(e, e->d_series, e->d_series_row);
+            if (err != cudaSuccess) return err;
+        }
+        cudaError_t err = m != e ? ym::launch_convert(e, m) : cudaSuccess;
+        if (err == cudaSuccess) err = ym::launch_wilson_loops(m, run->rmax, run->tmax, m->d_obs_partial, m->d_obs_out);
+        if (err == cudaSuccess)
+            err = ym::launch_store_rows(e->stream, m->d_obs_out, e->n_chains * 96, e->d_wilson_series, e->d_loop_row, 0);
+        if (err == cudaSuccess) err = ym::launch_polyakov(m, run->polyakov_direction, m->d_obs_partial, m->d_obs_out);
+        if (err == cudaSuccess)
+            err = ym::launch_store_rows(e->stream, m->d_obs_out, e->n_chains * 2, e->d_poly_series, e->d_loop_row, 1);
+        return err;
+    };
+    if (!e->run_graph || e->run_graph_angle != angle || e->run_graph_mode != mode || e->run_graph_sweeps != spb ||
+        e->run_graph_rmax != run->rmax || e->run_graph_tmax != run->tmax ||
+        e->run_graph_dir != run->polyakov_direction || e->run_graph_view != (const void *)m ||
+        e->run_graph_view_links != (const void *)m->d_links) {
+        drop_run_graph(e);
+        cudaGraph_t g = nullptr;
+        // the measurement handle's launches join the capture on e's stream
+        cudaStream_t saved = m->stream;
+        m->stream = e->stream;
+        cudaError_t err = cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal);
+        if (err == cudaSuccess) {
+            err = block();
+            const cudaError_t end = cudaStreamEndCapture(e->stream, &g);
+            if (err == cudaSuccess) err = end;
+        }
+        m->stream = saved;
+        if (err == cudaSuccess) err = cudaGraphInstantiate(&e->run_graph, g, 0);
+        if (g) cudaGraphDestroy(g);
+        YM_CUDA(err);
+        e->run_graph_angle = angle;
+        e->run_graph_mode = mode;
+        e->run_graph_sweeps = spb;
+        e->run_graph_rmax = run->rmax;
+        e->run_graph_tmax = run->tmax;
+        e->run_graph_dir = run->polyakov_direction;
+        e->run_graph_view = m;
+        e->run_graph_view_links = m->d_links;
+    }
+    for (int64_t b = 0; b < run->n_blocks; ++b) YM_CUDA(cudaGraphLaunch(e->run_graph, e->stream));
+    YM_CUDA(cudaMemcpyAsync(plaquette, e->d_series, (size_t)(rows * e->n_chains) * sizeof(double),
+                            cudaMemcpyDeviceToHost, e->stream));
+    YM_CUDA(cudaMemcpyAsync(wilson, e->d_wilson_series, (size_t)(run->n_blocks * e->n_chains * 96) * sizeof(double),
+                            cudaMemcpyDeviceToHost, e->stream));
+    YM_CUDA(cudaMemcpyAsync(polyakov, e->d_poly_series, (size_t)(run->n_blocks * e->n_chains * 2) * sizeof(double),
+                            cudaMemcpyDeviceToHost, e->stream));
+    YM_CUDA(cudaStreamSynchronize(e->stream));
+    for (int64_t ch = 0; ch < e->n_chains; ++ch)
+        e->proposals[ch] += (uint64_t)rows * 32u * (uint64_t)e->chains[ch].volume;
+    for (int64_t i = 0; i < rows * e->n_chains; ++i)
+        if (!std::isfinite(plaquette[i])) return YM_ERR_NON_FINITE_OBSERVABLE;
+    for (int64_t i = 0; i < run->n_blocks * e->n_chains * 96; ++i)
+        if (!std::isfinite(wilson[i])) return YM_ERR_NON_FINITE_OBSERVABLE;
+    for (int64_t i = 0; i < run->n_blocks * e->n_chains * 2; ++i)
+        if (!std::isfinite(polyakov[i])) return YM_ERR_NON_FINITE_OBSERVABLE;
+    return YM_OK;
+}
+
+int32_t ym_ensemble_lift_angle_cap(ym_ensemble *e, int32_t lift) {
+    if (!e) return YM_ERR_NULL_ARGUMENT;
+    if (lift && (e->group != YM_GROUP_SU3 || e->precision != YM_PREC_F32_TWO_ROW))
+        return YM_ERR_UNSUPPORTED_PRECISION;
+    e->angle_cap_lifted = lift != 0;
     return YM_OK;
 }
 
@@ -797,6 +959,45 @@ int32_t ym_su3_polyakov_loops(ym_ensemble *e, int32_t direction, double *out) {
     YM_CUDA(cudaMemcpyAsync(out, e->d_obs_out, (size_t)e->n_chains * 2 * sizeof(double),
                             cudaMemcpyDeviceToHost, e->stream));
     YM_CUDA(cudaStreamSynchronize(e->stream));
+    return YM_OK;
+}
+
+int32_t ym_su2_wilson_loops(ym_ensemble *e, int32_t rmax, int32_t tmax, double *out) {
+    if (!e || !out) return YM_ERR_NULL_ARGUMENT;
+    if (e->group != YM_GROUP_SU2) return YM_ERR_WRONG_GROUP;
+    if (e->precision != YM_PREC_F64) return YM_ERR_UNSUPPORTED_PRECISION;
+    if (rmax == 0 || tmax == 0) return YM_ERR_ZERO_RECTANGLE_EXTENT;   // lib.rs:452-454
+    if (rmax < 0 || tmax < 0 || rmax > 4 || tmax > 4) return YM_ERR_INVALID_ARGUMENT;
+    int32_t st = set_device(e);
+    if (st) return st;
+    YM_CUDA(ensure_obs_scratch(e));
+    YM_CUDA(timed(e, YM_KERNEL_AUX, [&] {
+        return ym::launch_su2_wilson_loops(e, rmax, tmax, e->d_obs_partial, e->d_obs_out);
+    }));
+    YM_CUDA(cudaMemcpyAsync(out, e->d_obs_out, (size_t)e->n_chains * 96 * sizeof(double),
+                            cudaMemcpyDeviceToHost, e->stream));
+    YM_CUDA(cudaStreamSynchronize(e->stream));
+    for (int64_t i = 0; i < e->n_chains * 96; ++i)
+        if (!std::isfinite(out[i])) return YM_ERR_NON_FINITE_OBSERVABLE;
+    return YM_OK;
+}
+
+int32_t ym_su2_polyakov_loops(ym_ensemble *e, int32_t direction, double *out) {
+    if (!e || !out) return YM_ERR_NULL_ARGUMENT;
+    if (e->group != YM_GROUP_SU2) return YM_ERR_WRONG_GROUP;
+    if (direction < 0 || direction >= 4) return YM_ERR_DIRECTION_OUT_OF_RANGE;
+    int32_t st = set_device(e);
+    if (st) return st;
+    YM_CUDA(ensure_obs_scratch(e));
+    YM_CUDA(timed(e, YM_KERNEL_AUX, [&] { return ym::launch_su2_polyakov(e, direction, e->d_obs_partial, e->d_obs_out); }));
+    std::vector<double> both((size_t)e->n_chains * 2);
+    YM_CUDA(cudaMemcpyAsync(both.data(), e->d_obs_out, both.size() * sizeof(double),
+                            cudaMemcpyDeviceToHost, e->stream));
+    YM_CUDA(cudaStreamSynchronize(e->stream));
+    for (int64_t ch = 0; ch < e->n_chains; ++ch) {
+        out[ch] = both[(size_t)ch * 2];
+        if (!std::isfinite(out[ch])) return YM_ERR_NON_FINITE_OBSERVABLE;
+    }
     return YM_OK;
 }
 

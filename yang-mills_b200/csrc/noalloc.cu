@@ -12,11 +12,13 @@
 // The array is a file-scope __device__ variable: every GPU that loads the
 // library holds it (512 KiB) until the process exits.  In host code its name
 // is only a host-side stand-in, never a device address, so the launcher
-// resolves the real address with cudaGetSymbolAddress once per device, on
-// that device's first call, and passes that pointer to the kernels.
+// resolves the real address with cudaGetSymbolAddress once per device (again
+// after a device reset, which gives the device a new context), on that
+// device's first call, and passes that pointer to the kernels.
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
 
 #include "ym_internal.hpp"
 
@@ -116,27 +118,79 @@ __global__ void k_plaquette_final(const double *partials, int64_t n, double volu
     if (threadIdx.x == 0) out[0] = v / (6.0 * volume);
 }
 
-// Device address of g_plaquette_partials, resolved once per device with that
-// device current.
-double *partials_address(int32_t *status) {
-    static double *cached[128] = {};
+// Driver entry points that name the calling thread's current context.  A
+// context's id is unique for the life of the process: after a device reset
+// the primary context is a new one, the library's module is loaded into it
+// again, and the array has a new device address.
+using CtxGetCurrentFn = int (*)(void **ctx);
+using CtxGetIdFn = int (*)(void *ctx, unsigned long long *id);
+
+struct ContextIds {
+    CtxGetCurrentFn get_current = nullptr;
+    CtxGetIdFn get_id = nullptr;
+};
+
+const ContextIds &context_ids() {
+    static const ContextIds ids = [] {
+        ContextIds c;
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            c.get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+        f = nullptr;
+        q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            c.get_id = reinterpret_cast<CtxGetIdFn>(f);
+        return c;
+    }();
+    return ids;
+}
+
+// Id of the current context; false when it cannot be told (no context
+// current yet, or the driver lacks the entry points).
+bool current_context_id(unsigned long long *id) {
+    const ContextIds &c = context_ids();
+    if (!c.get_current || !c.get_id) return false;
+    void *ctx = nullptr;
+    if (c.get_current(&ctx) != 0 || !ctx) return false;
+    return c.get_id(ctx, id) == 0;
+}
+
+// Device address of g_plaquette_partials in the current context, resolved by
+// cudaGetSymbolAddress with the caller's device current the first time a
+// context calls, then kept per device together with that context's id.  A
+// call from a later context (after a reset) resolves it again; when the
+// context cannot be identified every call resolves it.  The table is shared
+// by host threads and guarded by a mutex.
+struct ResolvedAddress {
+    unsigned long long context_id = 0;
+    double *ptr = nullptr;
+};
+std::mutex g_address_mutex;
+ResolvedAddress g_address[128];
+
+cudaError_t partials_address(double **out) {
     int dev = 0;
     cudaError_t err = cudaGetDevice(&dev);
-    if (err != cudaSuccess || dev < 0 || dev >= 128) {
-        *status = YM_ERR_CUDA;
-        return nullptr;
+    if (err != cudaSuccess) return err;
+    if (dev < 0 || dev >= 128) return cudaErrorInvalidDevice;
+    unsigned long long id = 0;
+    bool known = current_context_id(&id);
+    std::lock_guard<std::mutex> lock(g_address_mutex);
+    if (known && g_address[dev].ptr && g_address[dev].context_id == id) {
+        *out = g_address[dev].ptr;
+        return cudaSuccess;
     }
-    if (!cached[dev]) {
-        void *ptr = nullptr;
-        err = cudaGetSymbolAddress(&ptr, g_plaquette_partials);
-        if (err != cudaSuccess || !ptr) {
-            *status = YM_ERR_CUDA;
-            return nullptr;
-        }
-        cached[dev] = static_cast<double *>(ptr);
-    }
-    *status = YM_OK;
-    return cached[dev];
+    void *ptr = nullptr;
+    err = cudaGetSymbolAddress(&ptr, g_plaquette_partials);
+    if (err != cudaSuccess) return err;
+    if (!ptr) return cudaErrorInvalidSymbol;
+    known = current_context_id(&id);   // the lookup has made the context current
+    g_address[dev] = known ? ResolvedAddress{id, static_cast<double *>(ptr)} : ResolvedAddress{};
+    *out = static_cast<double *>(ptr);
+    return cudaSuccess;
 }
 
 }  // namespace
@@ -158,12 +212,18 @@ extern "C" int32_t ym_su3_average_plaquette_noalloc(const double *links, const i
     g.volume = sites;
     const int64_t tiles = (sites + kThreads - 1) / kThreads;
     if (tiles > kMaxTiles) return YM_ERR_SCRATCH_TOO_SMALL;
-    int32_t st = YM_OK;
-    double *partials = partials_address(&st);
-    if (st) return st;
+    double *partials = nullptr;
+    cudaError_t err = partials_address(&partials);
+    if (err != cudaSuccess) return ym::record_cuda_status(err);
+    // An error still pending from the caller's earlier work is reported as
+    // it is (and left pending) rather than blamed on these launches.
+    err = cudaPeekAtLastError();
+    if (err != cudaSuccess) return ym::record_cuda_status(err);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     k_plaquette_partials<<<(unsigned)tiles, kThreads, 0, s>>>(
         reinterpret_cast<const double2 *>(links), g, partials);
+    err = cudaGetLastError();
+    if (err != cudaSuccess) return ym::record_cuda_status(err);
     k_plaquette_final<<<1, 256, 0, s>>>(partials, tiles, (double)sites, out);
-    return cudaGetLastError() == cudaSuccess ? YM_OK : YM_ERR_CUDA;
+    return ym::record_cuda_status(cudaGetLastError());
 }

@@ -388,6 +388,12 @@ cudaError_t launch_wilson_loops(ym_ensemble *e, int rmax, int tmax, double *d_pa
     return cudaGetLastError();
 }
 
+cudaError_t launch_tile_mean(ym_ensemble *e, const double *d_partial, int width, int dir, double *d_out) {
+    k_tile_mean<<<dim3((unsigned)e->n_chains, (unsigned)width), 256, 0, e->stream>>>(
+        d_partial, e->d_site_tile_first, e->d_chains, width, dir, d_out);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_polyakov(ym_ensemble *e, int dir, double *d_partial, double *d_out) {
     k_polyakov<<<(unsigned)e->n_site_tiles, T, 0, e->stream>>>(e->d_chains, e->d_site_tiles, e->d_links,
                                                               dir, d_partial);

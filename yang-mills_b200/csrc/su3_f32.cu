@@ -180,6 +180,23 @@ __global__ void k_f32_to_aos(const ChainInfo *__restrict__ chains, int chain,
     }
 }
 
+// One link of a two-row chain as binary64 (the third row rebuilt, as
+// k_f32_to_aos writes it) / from binary64 (its first two rows rounded).
+__global__ void k_f32_get_link(const ChainInfo *__restrict__ chains, int chain, const float2 *links,
+                               int64_t s, int mu, double2 *out) {
+    const ChainInfo c = chains[chain];
+    const m3 u = load_as_f64(links, c, s, mu);
+    for (int e = 0; e < 9; ++e) out[e] = make_double2(u.e[e / 3][e % 3].re, u.e[e / 3][e % 3].im);
+}
+
+__global__ void k_f32_set_link(const ChainInfo *__restrict__ chains, int chain, float2 *links,
+                               int64_t s, int mu, const double2 *in) {
+    const ChainInfo c = chains[chain];
+    m3 u;
+    for (int e = 0; e < 9; ++e) u.e[e / 3][e % 3] = cmake(in[e].x, in[e].y);
+    store_rows_from_f64(links, c, s, mu, u);
+}
+
 // Two-row binary32 handle -> full binary64 handle of the same geometry.
 __global__ void __launch_bounds__(kSiteThreads)
 k_f32_to_f64(const ChainInfo *__restrict__ src_chains, const ChainInfo *__restrict__ dst_chains,
@@ -260,6 +277,16 @@ cudaError_t launch_f32_from_aos(ym_ensemble *e, int64_t chain) {
 cudaError_t launch_f32_to_aos(ym_ensemble *e, int64_t chain) {
     k_f32_to_aos<<<grid_for(e->chains[chain].volume, 128), 128, 0, e->stream>>>(
         e->d_chains, (int)chain, f32_links(e), reinterpret_cast<double2 *>(e->d_staging));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_f32_get_link(ym_ensemble *e, int64_t chain, int64_t s, int mu, double2 *out) {
+    k_f32_get_link<<<1, 1, 0, e->stream>>>(e->d_chains, (int)chain, f32_links(e), s, mu, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_f32_set_link(ym_ensemble *e, int64_t chain, int64_t s, int mu, const double2 *in) {
+    k_f32_set_link<<<1, 1, 0, e->stream>>>(e->d_chains, (int)chain, f32_links(e), s, mu, in);
     return cudaGetLastError();
 }
 

@@ -305,6 +305,22 @@ __global__ void k_store_series(const double *__restrict__ result, double *__rest
     if (threadIdx.x == 0) *counter = row + 1;
 }
 
+// dst[row * n + i] = src[i] for row = *counter; advance: *counter = row + 1
+// (one block; replayable inside a graph).
+__global__ void k_store_rows(const double *__restrict__ src, int64_t n, double *__restrict__ dst,
+                             uint64_t *__restrict__ counter, int advance) {
+    const uint64_t row = *counter;
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) dst[row * n + i] = src[i];
+    __syncthreads();
+    if (advance && threadIdx.x == 0) *counter = row + 1;
+}
+
+cudaError_t launch_store_rows(cudaStream_t st, const double *src, int64_t n, double *dst,
+                              uint64_t *counter, int advance) {
+    k_store_rows<<<1, 256, 0, st>>>(src, n, dst, counter, advance);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_store_series(ym_ensemble *e, double *series, uint64_t *counter) {
     k_store_series<<<1, 256, 0, e->stream>>>(e->d_result, series, counter, (int)e->n_chains);
     return cudaGetLastError();

@@ -18,6 +18,10 @@ constexpr int64_t kLpPartialStride = 6304;  // floats per tile of learned-propos
 // Groups of 64 tiles in the first stage of the gradient reduction.
 inline int64_t lp_reduce_groups(int64_t tiles) { return (tiles + 63) / 64; }
 
+// Maps a CUDA error onto a status (YM_OK or YM_ERR_CUDA) and records a
+// failure as the calling thread's ym_last_cuda_error (capi.cu).
+int32_t record_cuda_status(cudaError_t err);
+
 }  // namespace ym
 
 struct ym_ensemble {
@@ -67,6 +71,14 @@ struct ym_ensemble {
     int64_t n_slices = 0;
     double2 *d_links_tmp = nullptr;        // second link buffer (smearing levels)
 
+    // Lattice queries (lattice_ops.cu), allocated on first use.
+    unsigned *d_query_error = nullptr;     // error bits of the running query
+    double *d_query = nullptr;             // 64 doubles: single-site results and arguments
+    int32_t *d_steps = nullptr;            // a path's steps
+    int64_t steps_capacity = 0;
+    double *d_terms = nullptr;             // per-plaquette action terms of one chain
+    int64_t terms_capacity = 0;
+
     // Captured batch of sweeps, replayed by ym_su3_metropolis_sweeps (the
     // sweep index lives in device memory, so every replay advances it).
     cudaGraphExec_t sweep_graph = nullptr;
@@ -80,6 +92,21 @@ struct ym_ensemble {
     // Small-chain path choice: -1 not yet measured, 0 tiled launches, 1 the
     // chain-resident kernel (picked by timing both on the first sweeps).
     int32_t resident_choice = -1;
+    // Half widths above the reference's 1.0 admitted (two-row handles only).
+    bool angle_cap_lifted = false;
+    // Captured block of the loop-measurement cadence (ym_su3_measured_run):
+    // sweeps with a plaquette each, then Wilson and Polyakov loops.
+    cudaGraphExec_t run_graph = nullptr;
+    double run_graph_angle = 0.0;
+    int32_t run_graph_mode = -1;
+    int64_t run_graph_sweeps = -1;
+    int32_t run_graph_rmax = 0, run_graph_tmax = 0, run_graph_dir = -1;
+    const void *run_graph_view = nullptr;      // measurement handle and its buffers
+    const void *run_graph_view_links = nullptr;
+    double *d_wilson_series = nullptr;     // [block][chain][96]
+    double *d_poly_series = nullptr;       // [block][chain][2]
+    int64_t loop_capacity = 0;             // rows
+    uint64_t *d_loop_row = nullptr;
     double *d_series = nullptr;            // [measurement][chain]
     int64_t series_capacity = 0;           // rows
     uint64_t *d_series_row = nullptr;
@@ -149,6 +176,9 @@ cudaError_t launch_su3_hot_start(ym_ensemble *e);
 cudaError_t launch_chain_reduce(ym_ensemble *e, const double *partial, double *out, int mode,
                                 double per_site);
 cudaError_t launch_store_series(ym_ensemble *e, double *series, uint64_t *counter);
+// Row *counter of dst (rows of n doubles) = src; advance bumps the counter.
+cudaError_t launch_store_rows(cudaStream_t st, const double *src, int64_t n, double *dst,
+                              uint64_t *counter, int advance);
 
 // observables.cu / smear.cu
 cudaError_t launch_wilson_loops(ym_ensemble *e, int rmax, int tmax, double *d_partial, double *d_out);
@@ -158,6 +188,13 @@ cudaError_t launch_operator_basis(ym_ensemble *e, double2 *d_site_vals, const in
                                   double *d_rect);
 cudaError_t launch_stout_level(ym_ensemble *e, const double2 *in, double2 *out, double rho);
 cudaError_t launch_block(ym_ensemble *fine, ym_ensemble *coarse);
+// Per-chain means of tile partials [tile][width] (loops: / volume; dir >= 0:
+// / number of lines along dir), fixed order.
+cudaError_t launch_tile_mean(ym_ensemble *e, const double *d_partial, int width, int dir, double *d_out);
+
+// lattice_ops.cu (SU(2) lattice averages of the reference's loops)
+cudaError_t launch_su2_wilson_loops(ym_ensemble *e, int rmax, int tmax, double *d_partial, double *d_out);
+cudaError_t launch_su2_polyakov(ym_ensemble *e, int dir, double *d_partial, double *d_out);
 
 // su3_f32.cu (two-row binary32 storage)
 cudaError_t launch_f32_metropolis(ym_ensemble *e, int parity, int mu, double angle, int uniform);
@@ -168,6 +205,10 @@ cudaError_t launch_f32_hot_start(ym_ensemble *e);
 cudaError_t launch_f32_from_aos(ym_ensemble *e, int64_t chain);
 cudaError_t launch_f32_to_aos(ym_ensemble *e, int64_t chain);
 cudaError_t launch_convert(ym_ensemble *src, ym_ensemble *dst);
+// One link of a two-row handle as binary64 (9 double2, third row rebuilt) /
+// from binary64 (first two rows stored in binary32).
+cudaError_t launch_f32_get_link(ym_ensemble *e, int64_t chain, int64_t s, int mu, double2 *out);
+cudaError_t launch_f32_set_link(ym_ensemble *e, int64_t chain, int64_t s, int mu, const double2 *in);
 
 // su2.cu
 cudaError_t launch_su2_heatbath(ym_ensemble *e, int parity, int mu, int max_attempts, int kp);

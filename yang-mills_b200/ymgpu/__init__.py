@@ -9,10 +9,11 @@ a compute entry point without the built ``libymgpu.so`` raises.
 from ._lib import LIB_PATH, lib
 from .ensemble import Ensemble, F32_TWO_ROW, F64, ORDERED, SU2, SU3, UNIFORM
 from .errors import YmError
-from . import glueball, learned, su2_ensemble, su3_ensemble, su3_lattice
+from . import glueball, learned, path_holonomy, su2_ensemble, su3_ensemble, su3_lattice
 from .learned import ProposalModel
+from .lattice import Lattice4
 from .su3_lattice import Su3Lattice4
 
-__all__ = ["Ensemble", "Su3Lattice4", "YmError", "lib", "LIB_PATH", "su2_ensemble",
+__all__ = ["Ensemble", "Lattice4", "Su3Lattice4", "path_holonomy", "YmError", "lib", "LIB_PATH", "su2_ensemble",
            "su3_ensemble", "su3_lattice", "glueball", "SU2", "SU3", "F64", "F32_TWO_ROW", "ORDERED",
            "UNIFORM", "learned", "ProposalModel"]

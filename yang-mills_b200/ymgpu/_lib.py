@@ -23,6 +23,11 @@ class EnsembleDesc(C.Structure):
                 ("device", i32)]
 
 
+class MeasuredRun(C.Structure):
+    _fields_ = [("proposal_angle", f64), ("generator_mode", i32), ("polyakov_direction", i32),
+                ("n_blocks", i64), ("sweeps_per_block", i64), ("rmax", i32), ("tmax", i32)]
+
+
 # name -> (argtypes); every function returns int32 ym_status
 SIGNATURES = {
     "ym_last_cuda_error": [],
@@ -40,8 +45,10 @@ SIGNATURES = {
     "ym_su3_metropolis_sweeps": [VP, f64, i32, i64],
     "ym_su3_accounting": [VP, P(u64), P(u64)],
     "ym_ensemble_set_sweep_path": [VP, i32],
+    "ym_ensemble_lift_angle_cap": [VP, i32],
     "ym_ensemble_get_sweep_path": [VP, P(i32)],
     "ym_su3_measured_sweeps": [VP, f64, i32, i64, i64, P(f64)],
+    "ym_su3_measured_run": [VP, VP, P(MeasuredRun), P(f64), P(f64), P(f64)],
     "ym_reset_accounting": [VP],
     "ym_su3_reference_sweeps": [VP, f64, P(u64), i64, P(u64), P(u64)],
     "ym_su3_reference_average_plaquette": [VP, P(f64)],
@@ -51,6 +58,22 @@ SIGNATURES = {
     "ym_proposal_angle_from_u64": [u64, f64, P(f64)],
     "ym_su3_average_plaquette_noalloc": [VP, P(i64), VP, VP],
     "ym_su3_wilson_loops": [VP, i32, i32, P(f64)],
+    "ym_su2_wilson_loops": [VP, i32, i32, P(f64)],
+    "ym_su2_polyakov_loops": [VP, i32, P(f64)],
+    "ym_rectangular_path": [i32, i32, i64, i64, P(i32), i64, P(i64)],
+    "ym_path_holonomy": [VP, i64, P(i64), P(i32), i64, P(f64), P(i64)],
+    "ym_wilson_loop": [VP, i64, P(i64), P(i32), i64, P(f64)],
+    "ym_wilson_loop_sites": [VP, i64, P(i32), i64, P(f64)],
+    "ym_polyakov_loop": [VP, i64, P(i64), i32, P(f64)],
+    "ym_polyakov_loop_sites": [VP, i64, i32, P(f64)],
+    "ym_plaquette": [VP, i64, P(i64), i32, i32, P(f64)],
+    "ym_wilson_action": [VP, f64, P(f64)],
+    "ym_su2_staple": [VP, i64, P(i64), i32, P(f64), P(i64)],
+    "ym_su3_local_link_action": [VP, i64, P(i64), i32, f64, P(f64)],
+    "ym_su3_local_action_difference": [VP, i64, P(i64), i32, P(f64), f64, P(f64)],
+    "ym_su3_gauge_transform": [VP, i64, P(f64), VP, i64],
+    "ym_ensemble_get_link": [VP, i64, P(i64), i32, P(f64)],
+    "ym_ensemble_set_link": [VP, i64, P(i64), i32, P(f64)],
     "ym_su3_polyakov_loops": [VP, i32, P(f64)],
     "ym_su3_scalar_operator_basis": [VP, P(f64), P(f64)],
     "ym_ensemble_copy": [VP, VP],

@@ -14,7 +14,7 @@ from typing import Sequence
 
 import numpy as np
 
-from ._lib import EnsembleDesc, lib
+from ._lib import EnsembleDesc, MeasuredRun, lib
 from .errors import check
 
 SU2, SU3 = 2, 3
@@ -29,6 +29,18 @@ def _f64p(a: np.ndarray):
 
 def _u64p(a: np.ndarray):
     return a.ctypes.data_as(C.POINTER(C.c_uint64))
+
+
+def _i64p(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_int64))
+
+
+def _site(x) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(x, dtype=np.int64).reshape(4))
+
+
+def _steps(steps) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(steps, dtype=np.int32).reshape(-1))
 
 
 class Ensemble:
@@ -144,6 +156,30 @@ class Ensemble:
                                            _f64p(out)), "su3_measured_sweeps")
         return out
 
+    def measured_run(self, proposal_angle: float, n_blocks: int, sweeps_per_block: int = 10,
+                     rmax: int = 4, tmax: int = 4, polyakov_direction: int = 3,
+                     generator_mode="ordered", view: "Ensemble" = None):
+        """Sweeps with the plaquette after each, and Wilson (R x T <= rmax x tmax)
+        and Polyakov loops after every block of sweeps, one captured graph per
+        block (include/ymgpu.h ym_su3_measured_run).  A two-row handle needs
+        a binary64 ``view`` of the same extents for the loops.  Returns
+        (plaquette [sweep, chain], wilson [block, chain, plane, R-1, T-1],
+        polyakov [block, chain] complex)."""
+        run = MeasuredRun(float(proposal_angle), _GEN[generator_mode], int(polyakov_direction),
+                          int(n_blocks), int(sweeps_per_block), int(rmax), int(tmax))
+        plaq = np.zeros((n_blocks * sweeps_per_block, self.n_chains), np.float64)
+        wil = np.zeros((n_blocks, self.n_chains, 6, 4, 4), np.float64)
+        pol = np.zeros((n_blocks, self.n_chains, 2), np.float64)
+        check(lib().ym_su3_measured_run(self._h, view.handle if view is not None else None,
+                                        C.byref(run), _f64p(plaq), _f64p(wil), _f64p(pol)),
+              "su3_measured_run")
+        return plaq, wil, pol[..., 0] + 1j * pol[..., 1]
+
+    def lift_angle_cap(self, lift: bool = True) -> None:
+        """Admit half widths up to 2.5 on a two-row handle (past the
+        reference's 1.0), for plain Metropolis at a learned scale."""
+        check(lib().ym_ensemble_lift_angle_cap(self._h, int(lift)), "lift_angle_cap")
+
     @property
     def sweep_path(self) -> str:
         """'auto' (undecided), 'tiled' or 'resident' (include/ymgpu.h)."""
@@ -238,6 +274,126 @@ class Ensemble:
         for e in self.extents:
             out.append((p[k:k + e[3]].copy(), r[k:k + e[3]].copy()))
             k += e[3]
+        return out
+
+    # ------------------------------------------------------------ per-site / per-link queries
+    def _link_reals(self) -> int:
+        return 18 if self.group == SU3 else 4
+
+    def _as_link(self, a: np.ndarray):
+        """Host form of one link: (3, 3) complex128 (SU(3)) or 4 float64."""
+        return a.view(np.complex128).reshape(3, 3) if self.group == SU3 else a
+
+    def get_link(self, chain: int, x, mu: int) -> np.ndarray:
+        """One link, moved alone (Su3Lattice4::link su3_lattice.rs:153-155)."""
+        out = np.zeros(self._link_reals(), np.float64)
+        check(lib().ym_ensemble_get_link(self._h, chain, _i64p(_site(x)), mu, _f64p(out)), "get_link")
+        return self._as_link(out)
+
+    def set_link(self, chain: int, x, mu: int, value) -> None:
+        """Su3Lattice4::set_link (su3_lattice.rs:157-166): one link, moved alone."""
+        dt = np.complex128 if self.group == SU3 else np.float64
+        v = np.ascontiguousarray(np.asarray(value, dtype=dt)).reshape(-1).view(np.float64)
+        if v.size != self._link_reals():
+            raise ValueError("link value has the wrong size for the group")
+        check(lib().ym_ensemble_set_link(self._h, chain, _i64p(_site(x)), mu, _f64p(v)), "set_link")
+
+    def path_holonomy(self, chain: int, start, steps):
+        """(holonomy, end) of path_holonomy (path_holonomy.rs:132-161)."""
+        st = _steps(steps)
+        hol = np.zeros(self._link_reals(), np.float64)
+        end = np.zeros(4, np.int64)
+        check(lib().ym_path_holonomy(self._h, chain, _i64p(_site(start)),
+                                     st.ctypes.data_as(C.POINTER(C.c_int32)), st.size, _f64p(hol),
+                                     _i64p(end)), "path_holonomy")
+        return self._as_link(hol), tuple(int(v) for v in end)
+
+    def wilson_loop(self, chain: int, start, steps) -> complex:
+        """wilson_loop (path_holonomy.rs:172-181): (1/3) Tr (SU(3)) or (1/2) Re Tr (SU(2))."""
+        st = _steps(steps)
+        out = np.zeros(2, np.float64)
+        check(lib().ym_wilson_loop(self._h, chain, _i64p(_site(start)),
+                                   st.ctypes.data_as(C.POINTER(C.c_int32)), st.size, _f64p(out)),
+              "wilson_loop")
+        return complex(out[0], out[1])
+
+    def wilson_loop_sites(self, chain: int, steps) -> np.ndarray:
+        """wilson_loop from every site of the chain, lexicographic order (complex128)."""
+        st = _steps(steps)
+        out = np.zeros(2 * int(np.prod(self.extents[chain])), np.float64)
+        check(lib().ym_wilson_loop_sites(self._h, chain, st.ctypes.data_as(C.POINTER(C.c_int32)),
+                                         st.size, _f64p(out)), "wilson_loop_sites")
+        return out.view(np.complex128)
+
+    def polyakov_loop(self, chain: int, start, direction: int) -> complex:
+        """Su3Lattice4::polyakov_loop (su3_lattice.rs:202-212) / Lattice4::polyakov_loop."""
+        out = np.zeros(2, np.float64)
+        check(lib().ym_polyakov_loop(self._h, chain, _i64p(_site(start)), direction, _f64p(out)),
+              "polyakov_loop")
+        return complex(out[0], out[1])
+
+    def polyakov_loop_sites(self, chain: int, direction: int) -> np.ndarray:
+        out = np.zeros(2 * int(np.prod(self.extents[chain])), np.float64)
+        check(lib().ym_polyakov_loop_sites(self._h, chain, direction, _f64p(out)),
+              "polyakov_loop_sites")
+        return out.view(np.complex128)
+
+    def plaquette_at(self, chain: int, x, mu: int, nu: int) -> np.ndarray:
+        """plaquette(x, mu, nu): SU(3) matrix / SU(2) quaternion."""
+        out = np.zeros(self._link_reals(), np.float64)
+        check(lib().ym_plaquette(self._h, chain, _i64p(_site(x)), mu, nu, _f64p(out)), "plaquette")
+        return self._as_link(out)
+
+    def wilson_action(self, beta: float) -> np.ndarray:
+        """wilson_action(beta) of every chain, the reference's sequential sum."""
+        out = np.zeros(self.n_chains, np.float64)
+        check(lib().ym_wilson_action(self._h, float(beta), _f64p(out)), "wilson_action")
+        return out
+
+    def su2_staple(self, chain: int, x, mu: int):
+        """Lattice4::staple (lib.rs:507-546): (components, terms)."""
+        out = np.zeros(4, np.float64)
+        terms = C.c_int64()
+        check(lib().ym_su2_staple(self._h, chain, _i64p(_site(x)), mu, _f64p(out), C.byref(terms)),
+              "su2_staple")
+        return out, terms.value
+
+    def local_link_action(self, chain: int, x, mu: int, beta: float) -> float:
+        out = np.zeros(1, np.float64)
+        check(lib().ym_su3_local_link_action(self._h, chain, _i64p(_site(x)), mu, float(beta),
+                                             _f64p(out)), "local_link_action")
+        return float(out[0])
+
+    def local_action_difference(self, chain: int, x, mu: int, candidate, beta: float) -> float:
+        """local_action_difference (su3_ensemble.rs:319-334)."""
+        cand = np.ascontiguousarray(np.asarray(candidate, dtype=np.complex128)).reshape(-1).view(np.float64)
+        out = np.zeros(1, np.float64)
+        check(lib().ym_su3_local_action_difference(self._h, chain, _i64p(_site(x)), mu, _f64p(cand),
+                                                   float(beta), _f64p(out)),
+              "local_action_difference")
+        return float(out[0])
+
+    def gauge_transform(self, chain: int, site_gauges, dst: "Ensemble" = None,
+                        dst_chain: int = None) -> None:
+        """Su3Lattice4::gauge_transform (su3_lattice.rs:244-283) into dst (default: in place);
+        site_gauges is (V, 3, 3) complex128 in lexicographic site order."""
+        g = np.ascontiguousarray(np.asarray(site_gauges, dtype=np.complex128)).view(np.float64)
+        if g.size != int(np.prod(self.extents[chain])) * 18:
+            raise ValueError("one SU(3) gauge per site is needed")
+        dst = self if dst is None else dst
+        dst_chain = chain if dst_chain is None else dst_chain
+        check(lib().ym_su3_gauge_transform(self._h, chain, _f64p(g), dst.handle, dst_chain),
+              "gauge_transform")
+
+    def su2_wilson_loops(self, rmax: int = 4, tmax: int = 4) -> np.ndarray:
+        """[chain, plane, R-1, T-1] lattice means of Lattice4::rectangular_wilson_loop."""
+        out = np.zeros(self.n_chains * 96, np.float64)
+        check(lib().ym_su2_wilson_loops(self._h, rmax, tmax, _f64p(out)), "su2_wilson_loops")
+        return out.reshape(self.n_chains, 6, 4, 4)
+
+    def su2_polyakov_loops(self, direction: int = 3) -> np.ndarray:
+        out = np.zeros(self.n_chains, np.float64)
+        check(lib().ym_su2_polyakov_loops(self._h, direction, _f64p(out)), "su2_polyakov_loops")
         return out
 
     def reunitarize(self) -> None:

@@ -5,6 +5,13 @@ handle (every sub-sweep launch covers all of them), the run_chain cadence
 (su3_ensemble.rs:408-480) replayed from a captured graph, per-chain
 diagnostics through the reference estimator.
 
+``su3_measured_run`` / ``fp32_vs_fp64_run``: the loop-measurement cadence
+of large SU(3) lattices -- sweeps with the plaquette after every one, Wilson
+loops R x T <= 4 x 4 and Polyakov loops every block of sweeps, each block one
+captured graph -- in two-row binary32 (binary64 reunitarisation every sweep)
+or binary64 storage, and the binary32 run's error against a binary64 run of
+the same length from the same field, seeds and sweep indices.
+
 ``scalar_glueball_pipeline``: uneven chain groups in one handle, then per
 measurement spatial stout smearing at several level counts, stride-2
 blocking where the reference admits it (fine extent >= 6 and even), the A1++
@@ -21,7 +28,7 @@ from typing import Dict, List, Sequence, Tuple
 import numpy as np
 
 from . import glueball as G
-from .ensemble import F64, Ensemble
+from .ensemble import F32_TWO_ROW, F64, Ensemble
 from .su2_ensemble import diagnostics
 from .su3_ensemble import derive_su3_chain_seed
 
@@ -76,6 +83,116 @@ def batched_su3_chains(n_chains: int = 64, extents=(4, 4, 4, 4), beta: float = 6
         acceptance=float((a1 - a0).sum()) / float((p1 - p0).sum()),
         link_updates=int(n_chains * int(np.prod(extents)) * 4 * measurements * sweeps_per_measurement),
         seconds=secs)
+
+
+@dataclass
+class MeasuredRunResult:
+    extents: List[Tuple[int, ...]]
+    precision: int
+    sweeps_per_block: int
+    plaquette: np.ndarray              # [sweep, chain]
+    wilson: np.ndarray                 # [block, chain, plane, R-1, T-1]
+    polyakov: np.ndarray               # [block, chain] complex
+    seconds: float                     # the measured run (sweeps + loop measurements)
+    sweep_seconds: float               # the same number of sweeps with a plaquette each, no loops
+    link_updates: int
+
+    @property
+    def link_updates_per_s(self) -> float:
+        return self.link_updates / self.seconds
+
+    @property
+    def loop_measurement_seconds(self) -> float:
+        return max(0.0, self.seconds - self.sweep_seconds)
+
+
+def su3_measured_run(ens: Ensemble, n_blocks: int, sweeps_per_block: int = 10,
+                     proposal_angle: float = 0.3, generator_mode: str = "ordered",
+                     rmax: int = 4, tmax: int = 4, polyakov_direction: int = 3,
+                     view: Ensemble = None, time_sweeps_alone: bool = True) -> MeasuredRunResult:
+    """The loop-measurement cadence on an existing handle (its current field,
+    seeds and sweep index).  A two-row handle measures its loops through a
+    binary64 ``view`` (made here when not given).  With time_sweeps_alone the
+    same sweeps are timed once more without the loop measurements, from the
+    same starting state, to give the measurements' cost."""
+    own_view = view is None and ens.precision == F32_TWO_ROW
+    if own_view:
+        view = ens.like(precision=F64)
+    try:
+        start_sweep = ens.sweep_index
+        saved = None
+        if time_sweeps_alone:
+            saved = ens.like()
+            ens.copy_to(saved)
+            ens.synchronize()
+            t0 = time.perf_counter()
+            ens.measured_sweeps(proposal_angle, n_blocks * sweeps_per_block, 1, generator_mode)
+            sweep_secs = time.perf_counter() - t0
+            saved.copy_to(ens)
+            ens.sweep_index = start_sweep
+        ens.synchronize()
+        t0 = time.perf_counter()
+        plaq, wil, pol = ens.measured_run(proposal_angle, n_blocks, sweeps_per_block, rmax, tmax,
+                                          polyakov_direction, generator_mode, view=view)
+        secs = time.perf_counter() - t0
+        if saved is not None:
+            saved.close()
+    finally:
+        if own_view:
+            view.close()
+    links = int(sum(np.prod(e) * 4 for e in ens.extents))
+    return MeasuredRunResult([tuple(e) for e in ens.extents], ens.precision, sweeps_per_block, plaq,
+                             wil, pol, secs, sweep_secs if time_sweeps_alone else float("nan"),
+                             links * n_blocks * sweeps_per_block)
+
+
+@dataclass
+class PrecisionComparison:
+    fp32: MeasuredRunResult
+    fp64: MeasuredRunResult
+    plaquette_mean_fp32: float
+    plaquette_mean_fp64: float
+    plaquette_error: float             # |mean FP32 - mean FP64|
+    plaquette_combined_sigma: float    # combined standard error of the two means
+    first_sweep_plaquette_error: float # max over chains after the first sweep (same field, same streams)
+    wilson_max_error: float            # max |W_32 - W_64| over blocks, chains, planes, R, T
+    polyakov_max_error: float
+
+
+def fp32_vs_fp64_run(start: Ensemble, n_blocks: int, sweeps_per_block: int = 10,
+                     proposal_angle: float = 0.3, generator_mode: str = "ordered",
+                     max_lag: int = 20) -> PrecisionComparison:
+    """The cadence run twice from the binary64 field of ``start`` (its seeds
+    and sweep index): in two-row binary32 and in binary64.  Both runs start
+    from the same links (the binary32 copy rounds them), draw from the same
+    per-link streams and measure the same observables; the comparison states
+    the binary32 run's error against the binary64 one.  Trajectories of the
+    two runs separate after a few sweeps (Metropolis decisions near the
+    threshold flip), so the plaquette is compared as run means with their
+    combined standard error; the first sweep is compared directly."""
+    sweep = start.sweep_index
+    with start.like(precision=F32_TWO_ROW) as f32, start.like(precision=F64) as f64, \
+            start.like(precision=F64) as view:
+        start.convert_to(f32)
+        f32.sweep_index = sweep
+        start.copy_to(f64)
+        f64.sweep_index = sweep
+        r32 = su3_measured_run(f32, n_blocks, sweeps_per_block, proposal_angle, generator_mode, view=view)
+        r64 = su3_measured_run(f64, n_blocks, sweeps_per_block, proposal_angle, generator_mode)
+
+    def mean_err(series):
+        flat = series.mean(1)
+        lag = max(1, min(max_lag, len(flat) - 1))
+        d = diagnostics(flat, lag)[0]
+        return float(flat.mean()), float(d.standard_error)
+
+    m32, e32 = mean_err(r32.plaquette)
+    m64, e64 = mean_err(r64.plaquette)
+    return PrecisionComparison(
+        r32, r64, m32, m64, abs(m32 - m64), float(np.hypot(e32, e64)),
+        float(np.max(np.abs(r32.plaquette[0] - r64.plaquette[0]))),
+        float(np.max(np.abs(r32.wilson - r64.wilson))),
+        float(np.max(np.abs(r32.polyakov - r64.polyakov))))
 
 
 @dataclass

@@ -130,6 +130,17 @@ def metropolis_sweep(lattice: Su3Lattice4, beta: float, proposal_angle: float,
     return MetropolisAccounting(int(p1[0] - p0[0]), int(a1[0] - a0[0]))
 
 
+def local_link_action(lattice: Su3Lattice4, x, mu: int, beta: float) -> float:
+    """su3_ensemble.rs:311-317."""
+    return lattice.ensemble.local_link_action(0, x, mu, beta)
+
+
+def local_action_difference(lattice: Su3Lattice4, x, mu: int, candidate, beta: float) -> float:
+    """su3_ensemble.rs:319-334: S(candidate) - S(current) over the twelve
+    plaquettes holding link (x, mu)."""
+    return lattice.ensemble.local_action_difference(0, x, mu, candidate, beta)
+
+
 def average_plaquette(lattice: Su3Lattice4) -> float:
     return float(lattice.ensemble.average_plaquette()[0])
 

@@ -1,8 +1,9 @@
 """Device-resident ``Su3Lattice4`` -- mirror of the reference type
 (reference/rust/src/su3_lattice.rs:20-313).
 
-The links live on the GPU in the engine's structure-of-arrays layout; the
-accessors below move them in the reference's own order when a caller asks.
+The links live on the GPU in the engine's structure-of-arrays layout; every
+method evaluates on the device and moves only its result (one link for
+link/set_link, one matrix for plaquette, one number for the action).
 """
 from __future__ import annotations
 
@@ -13,10 +14,6 @@ import numpy as np
 from .ensemble import Ensemble
 
 DIM = 4
-
-
-def _site_index(extents, x) -> int:
-    return ((x[0] * extents[1] + x[1]) * extents[2] + x[2]) * extents[3] + x[3]
 
 
 class Su3Lattice4:
@@ -52,12 +49,50 @@ class Su3Lattice4:
         return self.ensemble.download(0)
 
     def link(self, x, mu: int) -> np.ndarray:
-        return self.links()[_site_index(self.extents(), x) * DIM + mu]
+        """su3_lattice.rs:153-155: one link (3, 3) complex128, moved alone."""
+        return self.ensemble.get_link(0, x, mu)
 
     def set_link(self, x, mu: int, value: np.ndarray) -> None:
-        a = self.links()
-        a[_site_index(self.extents(), x) * DIM + mu] = value
-        self.ensemble.upload(0, a)
+        """su3_lattice.rs:157-166: one link, moved alone."""
+        self.ensemble.set_link(0, x, mu, value)
+
+    def plaquette(self, x, mu: int, nu: int) -> np.ndarray:
+        """su3_lattice.rs:168-181 (checked products)."""
+        return self.ensemble.plaquette_at(0, x, mu, nu)
+
+    def polyakov_holonomy(self, start, direction: int) -> np.ndarray:
+        """su3_lattice.rs:185-200: the ordered product wrapping one extent."""
+        n = self.extents()[direction]
+        hol, _ = self.ensemble.path_holonomy(0, start, [direction + 1] * n)
+        return hol
+
+    def polyakov_loop(self, start, direction: int) -> complex:
+        """su3_lattice.rs:202-212: (1/3) Tr of the periodic holonomy."""
+        return self.ensemble.polyakov_loop(0, start, direction)
+
+    def wilson_action(self, beta: float) -> float:
+        """su3_lattice.rs:214-242 (the reference's sequential sum)."""
+        return float(self.ensemble.wilson_action(beta)[0])
+
+    def gauge_transform(self, omega) -> "Su3Lattice4":
+        """su3_lattice.rs:244-283: a new lattice with g(x) U_mu(x) g(x+mu)^dag;
+        omega is a callable x -> (3, 3) matrix or a (V, 3, 3) array of
+        per-site gauges in lexicographic order."""
+        ext = self.extents()
+        if callable(omega):
+            g = np.empty((self.site_count(), 3, 3), np.complex128)
+            k = 0
+            for x0 in range(ext[0]):
+                for x1 in range(ext[1]):
+                    for x2 in range(ext[2]):
+                        for x3 in range(ext[3]):
+                            g[k] = omega((x0, x1, x2, x3))
+                            k += 1
+        else:
+            g = np.asarray(omega, dtype=np.complex128)
+        out = Su3Lattice4(self.ensemble.like())
+        self.ensemble.gauge_transform(0, g, out.ensemble, 0)
+        return out
 
     def max_link_unitarity_residual(self) -> float:
         return float(self.ensemble.max_residuals()[0][0])
