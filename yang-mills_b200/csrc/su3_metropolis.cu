@@ -356,7 +356,222 @@ __device__ __forceinline__ unsigned visit(m3 &u, const double2 (*sa)[T], double 
     return accepted;
 }
 
-template <int MU>
+// ---- the reference's ordered hits, software-pipelined ---------------------
+// A hit has a link-independent half (its two stream words, the angle, the
+// rotation entries from the Taylor chain, the uniform) and a link-dependent
+// half (candidate rows, Re Tr against the staple, the decision).  visit()
+// runs them back to back, and the Taylor chain's early exits split the code
+// into many small blocks; here every hit's link-independent half is computed
+// while the previous hit's link-dependent half runs, both branch-free in one
+// straight-line block, so each link carries two independent dependency
+// chains instead of one.  The values are visit()'s, bit for bit:
+//   * taylor_fixed<K> evaluates K terms of taylor_chain's recurrence and adds
+//     term k only while no earlier term was at or below the 1e-18 cutoff.
+//     K is taken from the proposal half width a so that every admissible
+//     angle stops within K terms: |t_k| <= |h|^k / k! with |h| <= a/2 for
+//     generators 1..7 and |h| <= 0.5774 a (at most 0.5 after lambda8's
+//     halving) for generator 8; a <= 0.3 stops by k = 13 (0.1732^13/13! =
+//     2e-20), a <= 1 by k = 16 (0.5^16/16! = 7e-19).
+//   * the decision is accept_step's u < exp(-max(dS, 0)) (for m = 0,
+//     exp(-0) = 1 > u, as its explicit branch gives); the accepted rows are
+//     selected, not branched to.
+template <int K>
+__device__ __forceinline__ void taylor_fixed(double h, double &c, double &s) {
+    double t = 1.0;
+    c = 1.0;
+    s = 0.0;
+    bool done = false;
+#pragma unroll
+    for (int k = 1; k <= K; ++k) {
+        t = (t * h) * c_inv[k];
+        if ((k & 3) == 1) { const double v = s + t; s = done ? s : v; }
+        else if ((k & 3) == 2) { const double v = c - t; c = done ? c : v; }
+        else if ((k & 3) == 3) { const double v = s - t; s = done ? s : v; }
+        else { const double v = c + t; c = done ? c : v; }
+        done = done || fabs(t) <= kTermCutoff;
+    }
+}
+
+// lambda8_rotation with taylor_chain2's lockstep chains (stopping on the
+// larger term) evaluated for K terms; |theta| <= 1 needs at most one halving.
+template <int K>
+__device__ __forceinline__ void lambda8_fixed(double theta, cplx &e1, cplx &e2) {
+    const double d1 = (0.5 * kInvSqrt3) * theta;
+    const double d2 = (-kInvSqrt3) * theta;
+    const bool sq = fmax(fabs(d1), fabs(d2)) > 0.5;
+    const double sc = sq ? 0.5 : 1.0;
+    const double h1 = d1 * sc, h2 = d2 * sc;
+    double t1 = 1.0, t2 = 1.0, c1 = 1.0, s1 = 0.0, c2 = 1.0, s2 = 0.0;
+    bool done = false;
+#pragma unroll
+    for (int k = 1; k <= K; ++k) {
+        t1 = (t1 * h1) * c_inv[k];
+        t2 = (t2 * h2) * c_inv[k];
+        if ((k & 3) == 1) { const double a = s1 + t1, b = s2 + t2; s1 = done ? s1 : a; s2 = done ? s2 : b; }
+        else if ((k & 3) == 2) { const double a = c1 - t1, b = c2 - t2; c1 = done ? c1 : a; c2 = done ? c2 : b; }
+        else if ((k & 3) == 3) { const double a = s1 - t1, b = s2 - t2; s1 = done ? s1 : a; s2 = done ? s2 : b; }
+        else { const double a = c1 + t1, b = c2 + t2; c1 = done ? c1 : a; c2 = done ? c2 : b; }
+        done = done || fmax(fabs(t1), fabs(t2)) <= kTermCutoff;
+    }
+    e1 = cmake(c1, s1);
+    e2 = cmake(c2, s2);
+    const cplx q1 = cmul(e1, e1), q2 = cmul(e2, e2);
+    e1 = sq ? q1 : e1;
+    e2 = sq ? q2 : e2;
+}
+
+struct BlockPre {
+    double c, s, unif, nlog;
+};
+struct DiagPre {
+    cplx e1, e2;
+    double unif, nlog;
+};
+
+template <int K>
+__device__ __forceinline__ BlockPre pre_block(uint64_t key, int h, double angle) {
+    BlockPre p;
+    taylor_fixed<K>(0.5 * grid_angle(splitmix_at(key, (uint64_t)(2 * h)), angle), p.c, p.s);
+    p.unif = unit_from(splitmix_at(key, (uint64_t)(2 * h + 1)));
+#ifdef YM_METRO_LOG_DECISION
+    p.nlog = -log(p.unif);
+#endif
+    return p;
+}
+
+template <int K>
+__device__ __forceinline__ DiagPre pre_diag(uint64_t key, int h, double angle) {
+    DiagPre p;
+    lambda8_fixed<K>(grid_angle(splitmix_at(key, (uint64_t)(2 * h)), angle), p.e1, p.e2);
+    p.unif = unit_from(splitmix_at(key, (uint64_t)(2 * h + 1)));
+#ifdef YM_METRO_LOG_DECISION
+    p.nlog = -log(p.unif);
+#endif
+    return p;
+}
+
+// u < exp(-m).  With YM_METRO_LOG_DECISION it is decided from L = -log(u),
+// computed off the link's dependency chain: m <= L - eps accepts and
+// m >= L + eps rejects exactly as the test itself would (log and exp are
+// each within an ulp and |L| <= 37, so the 1e-12 margin keeps exp(-m) and u
+// apart by a factor of at least 1 + 1e-12); only inside the band
+// (probability ~1e-12 per hit) is exp evaluated.
+__device__ __forceinline__ bool decide(double m, double unif, double nlog) {
+#ifdef YM_METRO_LOG_DECISION
+    constexpr double kBand = 1e-12;
+    bool acc = m <= nlog - kBand;
+    const bool rej = m >= nlog + kBand;
+    if (!acc && !rej) acc = unif < exp(-m);
+    return acc;
+#else
+    (void)nlog;
+    return unif < exp(-m);
+#endif
+}
+
+// hit_block for a compile-time generator, decision by selects.
+template <int I0, int I1, int KIND>
+__device__ __forceinline__ void hit_block_sel(m3 &u, const double2 (*sa)[T], double rr[3], double &old_tr,
+                                              const BlockPre &p, double beta3, unsigned &accepted) {
+    const double c = p.c, s = p.s;
+    cplx n0[3], n1[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const double x0 = u.e[I0][k].re, y0 = u.e[I0][k].im;
+        const double x1 = u.e[I1][k].re, y1 = u.e[I1][k].im;
+        if (KIND == 0) {
+            n0[k] = cmake(c * x0 - s * y1, c * y0 + s * x1);
+            n1[k] = cmake(c * x1 - s * y0, s * x0 + c * y1);
+        } else if (KIND == 1) {
+            n0[k] = cmake(c * x0 + s * x1, c * y0 + s * y1);
+            n1[k] = cmake(c * x1 - s * x0, c * y1 - s * y0);
+        } else {
+            n0[k] = cmake(c * x0 - s * y0, c * y0 + s * x0);
+            n1[k] = cmake(c * x1 + s * y1, c * y1 - s * x1);
+        }
+    }
+    cplx col0[3], col1[3];
+    sa_col(sa, I0, col0);
+    sa_col(sa, I1, col1);
+    double q[3] = {rr[0], rr[1], rr[2]};
+    q[I0] = retr_row_fma(n0, col0);
+    q[I1] = retr_row_fma(n1, col1);
+    const double new_tr = (q[0] + q[1]) + q[2];
+    const double m = fmax(beta3 * (old_tr - new_tr), 0.0);
+    const bool acc = decide(m, p.unif, p.nlog);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        u.e[I0][k] = acc ? n0[k] : u.e[I0][k];
+        u.e[I1][k] = acc ? n1[k] : u.e[I1][k];
+    }
+    rr[I0] = acc ? q[I0] : rr[I0];
+    rr[I1] = acc ? q[I1] : rr[I1];
+    old_tr = acc ? new_tr : old_tr;
+    accepted += acc ? 1u : 0u;
+}
+
+__device__ __forceinline__ void hit_diag_sel(m3 &u, const double2 (*sa)[T], double rr[3], double &old_tr,
+                                             const DiagPre &p, double beta3, unsigned &accepted) {
+    cplx n[3][3];
+    double q[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const cplx e = i < 2 ? p.e1 : p.e2;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) n[i][k] = cmul(e, u.e[i][k]);
+        cplx col[3];
+        sa_col(sa, i, col);
+        q[i] = retr_row_fma(n[i], col);
+    }
+    const double new_tr = (q[0] + q[1]) + q[2];
+    const double m = fmax(beta3 * (old_tr - new_tr), 0.0);
+    const bool acc = decide(m, p.unif, p.nlog);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) u.e[i][k] = acc ? n[i][k] : u.e[i][k];
+        rr[i] = acc ? q[i] : rr[i];
+    }
+    old_tr = acc ? new_tr : old_tr;
+    accepted += acc ? 1u : 0u;
+}
+
+// The eight ordered hits (generators 1..8, su3_ensemble.rs:361): hit h+1's
+// link-independent half is written next to hit h.
+template <int K>
+__device__ __forceinline__ unsigned visit_ordered(m3 &u, const double2 (*sa)[T], double beta3,
+                                                  double angle, uint64_t key) {
+    double rr[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        cplx col[3];
+        sa_col(sa, i, col);
+        rr[i] = retr_row_fma(u.e[i], col);
+    }
+    double old_tr = (rr[0] + rr[1]) + rr[2];
+    unsigned accepted = 0;
+    const BlockPre p0 = pre_block<K>(key, 0, angle);
+    const BlockPre p1 = pre_block<K>(key, 1, angle);
+    hit_block_sel<0, 1, 0>(u, sa, rr, old_tr, p0, beta3, accepted);
+    const BlockPre p2 = pre_block<K>(key, 2, angle);
+    hit_block_sel<0, 1, 1>(u, sa, rr, old_tr, p1, beta3, accepted);
+    const BlockPre p3 = pre_block<K>(key, 3, angle);
+    hit_block_sel<0, 1, 2>(u, sa, rr, old_tr, p2, beta3, accepted);
+    const BlockPre p4 = pre_block<K>(key, 4, angle);
+    hit_block_sel<0, 2, 0>(u, sa, rr, old_tr, p3, beta3, accepted);
+    const BlockPre p5 = pre_block<K>(key, 5, angle);
+    hit_block_sel<0, 2, 1>(u, sa, rr, old_tr, p4, beta3, accepted);
+    const BlockPre p6 = pre_block<K>(key, 6, angle);
+    hit_block_sel<1, 2, 0>(u, sa, rr, old_tr, p5, beta3, accepted);
+    const DiagPre p7 = pre_diag<K>(key, 7, angle);
+    hit_block_sel<1, 2, 1>(u, sa, rr, old_tr, p6, beta3, accepted);
+    hit_diag_sel(u, sa, rr, old_tr, p7, beta3, accepted);
+    return accepted;
+}
+
+// K: 0 = visit() (drawn generators); 13 / 16 = visit_ordered for half
+// widths <= 0.3 / <= 1.
+template <int MU, int K>
 __global__ void __launch_bounds__(T, YM_METRO_MIN_BLOCKS)
 k_su3_metropolis(const ChainInfo *__restrict__ chains, const Tile *__restrict__ tiles,
                  double2 *__restrict__ links, int parity, double angle, int uniform,
@@ -381,7 +596,8 @@ k_su3_metropolis(const ChainInfo *__restrict__ chains, const Tile *__restrict__ 
         cp_async_wait_all();
         m3 u = staged_link(bufs.l1);
         const uint64_t key = link_key(c.seed, sweep, x.lex, MU);
-        accepted = visit(u, sa, c.beta / 3.0, angle, key, uniform);
+        accepted = K ? visit_ordered<K>(u, sa, c.beta / 3.0, angle, key)
+                     : visit(u, sa, c.beta / 3.0, angle, key, uniform);
         store_su3(links, c, s, MU, u);
     }
     const unsigned warp_sum = __reduce_add_sync(0xffffffffu, accepted);
@@ -708,13 +924,28 @@ __global__ void k_advance_sweep(uint64_t *sweep) { *sweep += 1; }
 
 constexpr size_t kStageBytes = 27 * T * sizeof(double2);   // three staged factors per thread
 
+template <int K>
+static void metro_launch(ym_ensemble *e, int parity, int mu, double angle, int uniform) {
+    const dim3 grid((unsigned)e->n_half_tiles), block(T);
+    switch (mu) {
+    case 0: k_su3_metropolis<0, K><<<grid, block, kStageBytes, e->stream>>>(e->d_chains, e->d_half_tiles, e->d_links, parity, angle, uniform, e->d_sweep, e->d_accepts); break;
+    case 1: k_su3_metropolis<1, K><<<grid, block, kStageBytes, e->stream>>>(e->d_chains, e->d_half_tiles, e->d_links, parity, angle, uniform, e->d_sweep, e->d_accepts); break;
+    case 2: k_su3_metropolis<2, K><<<grid, block, kStageBytes, e->stream>>>(e->d_chains, e->d_half_tiles, e->d_links, parity, angle, uniform, e->d_sweep, e->d_accepts); break;
+    default: k_su3_metropolis<3, K><<<grid, block, kStageBytes, e->stream>>>(e->d_chains, e->d_half_tiles, e->d_links, parity, angle, uniform, e->d_sweep, e->d_accepts); break;
+    }
+}
+
 cudaError_t launch_su3_metropolis(ym_ensemble *e, int parity, int mu, double angle, int uniform) {
     static thread_local int configured_device = -1;
     int dev = 0;
     cudaGetDevice(&dev);
     if (configured_device != dev) {
-        const void *fns[4] = {(const void *)k_su3_metropolis<0>, (const void *)k_su3_metropolis<1>,
-                              (const void *)k_su3_metropolis<2>, (const void *)k_su3_metropolis<3>};
+        const void *fns[12] = {(const void *)k_su3_metropolis<0, 0>, (const void *)k_su3_metropolis<1, 0>,
+                               (const void *)k_su3_metropolis<2, 0>, (const void *)k_su3_metropolis<3, 0>,
+                               (const void *)k_su3_metropolis<0, 13>, (const void *)k_su3_metropolis<1, 13>,
+                               (const void *)k_su3_metropolis<2, 13>, (const void *)k_su3_metropolis<3, 13>,
+                               (const void *)k_su3_metropolis<0, 16>, (const void *)k_su3_metropolis<1, 16>,
+                               (const void *)k_su3_metropolis<2, 16>, (const void *)k_su3_metropolis<3, 16>};
         for (const void *f : fns) {
             cudaError_t err = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageBytes);
             if (err == cudaSuccess)
@@ -724,13 +955,11 @@ cudaError_t launch_su3_metropolis(ym_ensemble *e, int parity, int mu, double ang
         }
         configured_device = dev;
     }
-    const dim3 grid((unsigned)e->n_half_tiles), block(T);
-    switch (mu) {
-    case 0: k_su3_metropolis<0><<<grid, block, kStageBytes, e->stream>>>(e->d_chains, e->d_half_tiles, e->d_links, parity, angle, uniform, e->d_sweep, e->d_accepts); break;
-    case 1: k_su3_metropolis<1><<<grid, block, kStageBytes, e->stream>>>(e->d_chains, e->d_half_tiles, e->d_links, parity, angle, uniform, e->d_sweep, e->d_accepts); break;
-    case 2: k_su3_metropolis<2><<<grid, block, kStageBytes, e->stream>>>(e->d_chains, e->d_half_tiles, e->d_links, parity, angle, uniform, e->d_sweep, e->d_accepts); break;
-    default: k_su3_metropolis<3><<<grid, block, kStageBytes, e->stream>>>(e->d_chains, e->d_half_tiles, e->d_links, parity, angle, uniform, e->d_sweep, e->d_accepts); break;
-    }
+    // ordered hits: the pipelined visit with the term count the half width
+    // allows (angles are validated to lie in [1e-8, 1] for binary64 handles)
+    if (uniform) metro_launch<0>(e, parity, mu, angle, uniform);
+    else if (angle <= 0.3) metro_launch<13>(e, parity, mu, angle, uniform);
+    else metro_launch<16>(e, parity, mu, angle, uniform);
     return cudaGetLastError();
 }
 
