@@ -349,7 +349,8 @@ int32_t ym_ensemble_copy_chains(ym_ensemble *src, int64_t src_first, ym_ensemble
 /* spatial_stout_smear (glueball_smearing.rs:257-268): `levels` synchronous
  * spatial stout levels of src written to dst (same extents); rho in
  * (0, 0.25], levels <= 8 unless lift_level_cap (sequential levels compose,
- * so 10 = 8 then 2 exactly). */
+ * so 10 = 8 then 2 exactly).  dst may be src (smearing in place, so a
+ * caller measuring after 0, 5 and 10 levels smears 5 + 5, not 15). */
 int32_t ym_su3_spatial_stout_smear(ym_ensemble *src, ym_ensemble *dst, double rho, int64_t levels,
                                    int32_t lift_level_cap);
 /* spatial_stride2_block (glueball_blocking.rs:105-136): dst holds the

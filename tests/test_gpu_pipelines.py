@@ -83,3 +83,22 @@ def test_copy_of_consecutive_chains(oracle):
         finally:
             sub.close()
 
+
+
+def test_stout_in_place_continues_levels(oracle):
+    """Smearing in place continues the level sequence: 5 + 2 + 3 levels (odd
+    counts route through the second buffer) equal 10 levels from scratch
+    bit for bit."""
+    import ymgpu
+    exts = [[4, 4, 4, 6], [6, 6, 6, 4]]
+    with ymgpu.Ensemble(exts, 5.7, [1, 2]) as src:
+        src.hot_start()
+        src.metropolis_sweeps(1.0, 4, "uniform")
+        with src.like() as ref, src.like() as inc:
+            src.stout_smear_into(ref, 0.1, 10, lift_level_cap=True)
+            src.copy_to(inc)
+            inc.stout_smear_into(inc, 0.1, 5, lift_level_cap=True)
+            inc.stout_smear_into(inc, 0.1, 2, lift_level_cap=True)
+            inc.stout_smear_into(inc, 0.1, 3, lift_level_cap=True)
+            for c in range(2):
+                assert np.array_equal(inc.download(c), ref.download(c))

@@ -1101,10 +1101,18 @@ int32_t ym_su3_spatial_stout_smear(ym_ensemble *src, ym_ensemble *dst, double rh
     if (!same_geometry(src, dst)) return YM_ERR_LATTICE_EXTENTS_MISMATCH;
     st = set_device(dst);
     if (st) return st;
-    if (levels == 0) return ym_ensemble_copy(src, dst);
+    if (levels == 0) return src == dst ? YM_OK : ym_ensemble_copy(src, dst);
     if (!dst->d_links_tmp) YM_CUDA(dalloc(&dst->d_links_tmp, (size_t)dst->total_elems));
     YM_CUDA(cudaStreamSynchronize(src->stream));
     const double2 *in = src->d_links;
+    // Levels alternate between dst's two buffers and end in its links.  In
+    // place (src == dst) with an odd count the first level would write the
+    // buffer it reads, so the input moves to the second buffer first.
+    if (src == dst && levels % 2 == 1) {
+        YM_CUDA(cudaMemcpyAsync(dst->d_links_tmp, dst->d_links, (size_t)dst->total_elems * sizeof(double2),
+                                cudaMemcpyDeviceToDevice, dst->stream));
+        in = dst->d_links_tmp;
+    }
     for (int64_t k = 1; k <= levels; ++k) {
         double2 *out = ((levels - k) % 2 == 0) ? dst->d_links : dst->d_links_tmp;
         YM_CUDA(timed(dst, YM_KERNEL_STOUT, [&] { return ym::launch_stout_level(dst, in, out, rho); }));

@@ -260,8 +260,15 @@ def scalar_glueball_pipeline(groups: Sequence[Tuple[int, Sequence[int]]] = ((128
                 ens.synchronize()
                 t1 = time.perf_counter()
                 res.sweep_seconds += t1 - t0
-                for levels in stout_levels:
-                    ens.stout_smear_into(sm, rho, levels, lift_level_cap=True)
+                # levels are sequential, so each count continues from the
+                # previous one (0, 5, 10 costs 10 levels, not 15), bit for
+                # bit the same links as smearing from scratch
+                ens.copy_to(sm)
+                done = 0
+                for levels in sorted(stout_levels):
+                    if levels > done:
+                        sm.stout_smear_into(sm, rho, levels - done, lift_level_cap=True)
+                        done = levels
                     basis = sm.scalar_operator_basis()
                     for gi, chains in enumerate(per_group):
                         samples.setdefault((gi, levels, False), []).extend(basis[c] for c in chains)
