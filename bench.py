@@ -562,6 +562,7 @@ def main():
         s1 = e1.measured_sweeps(ANGLE, 1000, 1, "uniform")
         secs = time.perf_counter() - t
         path = e1.sweep_path
+        layout = e1.sweep_layout
         e1.close()
         d1 = [diagnostics(s1[:, c], 100)[0] for c in range(64)]
         m1 = s1.mean(0)
@@ -570,9 +571,10 @@ def main():
             "plaquette_ess_per_s": world * sum(d.effective_sample_size for d in d1) / secs,
             "tau_int": float(np.mean([d.integrated_autocorrelation_time for d in d1])),
             "plaquette_mean": float(m1.mean()), "plaquette_error": float(m1.std(ddof=1) / 8.0),
-            "sweep_path": path,
+            "sweep_path": path, "sweep_layout": layout,
             "note": "1000 measured sweeps (plaquette each) after 1000 at half width 1.0; one handle, "
-                    "graph-replayed or chain-resident as the handle's tuner chose"}
+                    "graph-replayed or chain-resident, and the sub-sweep layout, as the handle's "
+                    "tuner chose"}
         # scalar-glueball pipeline, batched uneven chains, beta=5.7
         from ymgpu.pipelines import scalar_glueball_pipeline
         t = time.perf_counter()
@@ -582,10 +584,11 @@ def main():
         out["glueball_pipeline_128x4^3x10+64x6^3x12+32x8^3x16"] = {
             "seconds": secs, "sweep_seconds": r.sweep_seconds, "measure_seconds": r.measure_seconds,
             "link_updates_per_s_in_sweeps": r.link_updates / r.sweep_seconds,
-            "surfaces": len(r.surfaces),
-            "note": "64 thermalisation sweeps, 4 measurements 4 sweeps apart; each measurement "
-                    "stout 0/5/10 levels (rho 0.1), stride-2 blocking of the 6^3 and 8^3 groups, "
-                    "A1++ operators; correlators, jackknife and covariance on the host"}
+            "surfaces": len(r.surfaces), "sweep_layout": r.sweep_layout, "sweep_path": r.sweep_path,
+            "note": "64 thermalisation sweeps (the first 50 probe the sub-sweep layouts), "
+                    "4 measurements 4 sweeps apart; each measurement stout 0/5/10 levels (rho 0.1, "
+                    "smeared incrementally: 10 levels in all), stride-2 blocking of the 6^3 and 8^3 "
+                    "groups, A1++ operators; correlators, jackknife and covariance on the host"}
         # the reference's phase-3F production campaign (16 x 4^3x10, beta 5.7) with
         # its correlated fits, and the published-baseline acceptance harnesses
         from ymgpu import benchmarks as B

@@ -148,6 +148,19 @@ enum { YM_PATH_AUTO = -1, YM_PATH_TILED = 0, YM_PATH_RESIDENT = 1 };
 int32_t ym_ensemble_set_sweep_path(ym_ensemble *ens, int32_t path);
 /* The path in use: YM_PATH_AUTO while not yet decided. */
 int32_t ym_ensemble_get_sweep_path(ym_ensemble *ens, int32_t *path);
+/* Work layout of the tiled SU(3) FP64 sub-sweep (no reference counterpart):
+ * the half lattice of every chain is cut into work items of item_sites
+ * sites (128, 64 or 32; a 128-thread CTA takes 128 / item_sites items, so
+ * the remainders of small chains share CTAs instead of leaving threads idle),
+ * listed in chain order (by_volume = 0) or largest chains first (1).  On a
+ * handle with several chains the first ym_su3_metropolis_sweeps call of at
+ * least 50 sweeps times 4 sweeps on each of the six layouts and keeps the
+ * fastest (then the chain-resident path is weighed against it as before);
+ * item_sites = 0 asks for that tuning again.  Every layout gives the same
+ * bits. */
+int32_t ym_ensemble_set_sweep_layout(ym_ensemble *ens, int32_t item_sites, int32_t by_volume);
+int32_t ym_ensemble_get_sweep_layout(ym_ensemble *ens, int32_t *item_sites, int32_t *by_volume,
+                                     int32_t *tuned);
 
 /* Proposal half widths above the reference's cap of 1.0 (no reference
  * counterpart: su3_ensemble.rs:28 rejects them).  With lift != 0 the sweeps

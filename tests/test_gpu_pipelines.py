@@ -102,3 +102,38 @@ def test_stout_in_place_continues_levels(oracle):
             inc.stout_smear_into(inc, 0.1, 3, lift_level_cap=True)
             for c in range(2):
                 assert np.array_equal(inc.download(c), ref.download(c))
+
+
+def test_sweep_layouts_give_the_same_bits_and_the_tuner_picks_one(oracle):
+    """Every sub-sweep layout (items of 128, 64 or 32 sites; chain order or
+    largest chains first) gives the same links and accept counts on uneven
+    chains; the tuner runs on the first call of >= 50 sweeps and reports its
+    choice, and its probe sweeps are ordinary sweeps (same bits as a fixed
+    layout)."""
+    import ymgpu
+    from ymgpu.su3_ensemble import derive_su3_chain_seed
+    exts = [[4, 4, 4, 10]] * 3 + [[6, 6, 6, 4]] * 2 + [[2, 4, 4, 6]]
+    seeds = [derive_su3_chain_seed(9, i) for i in range(len(exts))]
+    ref = None
+    for item in (128, 64, 32):
+        for by_volume in (False, True):
+            with ymgpu.Ensemble(exts, 5.7, seeds) as e:
+                e.set_sweep_layout(item, by_volume)
+                e.metropolis_sweeps(0.35, 5, "ordered")
+                e.metropolis_sweeps(0.35, 3, "uniform")
+                got = ([e.download(c) for c in range(len(exts))], e.accounting()[1])
+                assert e.sweep_layout == {"item_sites": item, "by_volume": by_volume, "tuned": True}
+            if ref is None:
+                ref = got
+            else:
+                assert all(np.array_equal(a, b) for a, b in zip(got[0], ref[0]))
+                assert np.array_equal(got[1], ref[1])
+    with ymgpu.Ensemble(exts, 5.7, seeds) as a, ymgpu.Ensemble(exts, 5.7, seeds) as b:
+        assert not a.sweep_layout["tuned"]
+        a.metropolis_sweeps(0.35, 100, "ordered")
+        assert a.sweep_layout["tuned"] and a.sweep_layout["item_sites"] in (128, 64, 32)
+        b.set_sweep_layout(128, False)
+        b.metropolis_sweeps(0.35, 100, "ordered")
+        for c in range(len(exts)):
+            assert np.array_equal(a.download(c), b.download(c))
+        assert np.array_equal(a.accounting()[1], b.accounting()[1])

@@ -6,6 +6,7 @@
 // enqueued on the handle's stream and synchronised before results return.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -75,6 +76,8 @@ void free_all(ym_ensemble *e) {
                     e->d_links_tmp, e->d_query_error, e->d_query, e->d_steps, e->d_terms};
     for (void *p : ptrs)
         if (p) cudaFree(p);
+    for (auto &l : e->layouts)
+        if (l.d_items) cudaFree(l.d_items);
     if (e->stream) cudaStreamDestroy(e->stream);
 }
 
@@ -243,6 +246,23 @@ bool resident_candidate(const ym_ensemble *e) {
 }
 
 constexpr int64_t kTuneSweeps = 4;   // sweeps timed per path when choosing
+// Sweeps a call needs before the layout tuner runs: its probes (one warm
+// sweep, then kTuneSweeps per layout, all ordinary sweeps of the chains
+// launched without graph replay) are then at most half of the call.
+constexpr int64_t kLayoutTuneMin = 2 * (ym::kSweepLayouts * kTuneSweeps + 1);
+
+// Selects sub-sweep layout li; captured graphs hold the previous layout's
+// launches, so they are dropped when it changes.
+void set_layout(ym_ensemble *e, int32_t li) {
+    if (e->sweep_layout == li && e->layout_tuned) return;
+    e->sweep_layout = li;
+    if (e->sweep_graph) cudaGraphExecDestroy(e->sweep_graph);
+    e->sweep_graph = nullptr;
+    if (e->measure_graph) cudaGraphExecDestroy(e->measure_graph);
+    e->measure_graph = nullptr;
+    if (e->run_graph) cudaGraphExecDestroy(e->run_graph);
+    e->run_graph = nullptr;
+}
 
 }  // namespace
 
@@ -331,6 +351,29 @@ int32_t ym_ensemble_create(const ym_ensemble_desc *desc, ym_ensemble **out) {
     }
     e->n_half_tiles = (int64_t)half.size();
     e->n_site_tiles = (int64_t)site.size();
+    // Sub-sweep layouts of the SU(3) FP64 sweep: work items of 128, 64 or 32
+    // sites, in chain order or with the largest chains first; a CTA takes
+    // 128 / item sites items, padded with chain = -1 items.
+    std::vector<std::vector<Tile>> lay(ym::kSweepLayouts);
+    {
+        std::vector<int64_t> chain_order((size_t)e->n_chains), by_volume;
+        for (int64_t ch = 0; ch < e->n_chains; ++ch) chain_order[(size_t)ch] = ch;
+        by_volume = chain_order;
+        std::stable_sort(by_volume.begin(), by_volume.end(), [&](int64_t a, int64_t b) {
+            return e->chains[(size_t)a].volume > e->chains[(size_t)b].volume;
+        });
+        for (int li = 0; li < ym::kSweepLayouts; ++li) {
+            const int log2 = 7 - li / 2;
+            const int64_t g = int64_t(1) << log2, per = ym::kSweepThreads / g;
+            for (int64_t ch : (li % 2) ? by_volume : chain_order)
+                for (int64_t s0 = 0; s0 < e->chains[(size_t)ch].half; s0 += g)
+                    lay[(size_t)li].push_back(Tile{(int32_t)ch, 0, s0});
+            while ((int64_t)lay[(size_t)li].size() % per) lay[(size_t)li].push_back(Tile{-1, 0, 0});
+            e->layouts[li].ctas = (int64_t)lay[(size_t)li].size() / per;
+            e->layouts[li].log2_item = log2;
+            e->layouts[li].by_volume = li % 2;
+        }
+    }
 
     cudaError_t err = cudaSetDevice(e->device);
     if (err == cudaSuccess) err = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
@@ -355,6 +398,12 @@ int32_t ym_ensemble_create(const ym_ensemble_desc *desc, ym_ensemble **out) {
         err = cudaMemcpy(e->d_chains, e->chains.data(), e->chains.size() * sizeof(ChainInfo), cudaMemcpyHostToDevice);
     if (err == cudaSuccess && !half.empty())
         err = cudaMemcpy(e->d_half_tiles, half.data(), half.size() * sizeof(Tile), cudaMemcpyHostToDevice);
+    for (int li = 0; li < ym::kSweepLayouts && err == cudaSuccess; ++li) {
+        err = dalloc(&e->layouts[li].d_items, lay[(size_t)li].size());
+        if (err == cudaSuccess && !lay[(size_t)li].empty())
+            err = cudaMemcpy(e->layouts[li].d_items, lay[(size_t)li].data(), lay[(size_t)li].size() * sizeof(Tile),
+                             cudaMemcpyHostToDevice);
+    }
     if (err == cudaSuccess && !site.empty())
         err = cudaMemcpy(e->d_site_tiles, site.data(), site.size() * sizeof(Tile), cudaMemcpyHostToDevice);
     if (err == cudaSuccess && !mixed.empty())
@@ -516,10 +565,37 @@ int32_t ym_su3_metropolis_sweeps(ym_ensemble *e, double angle, int32_t generator
         return ym::launch_advance_sweep(e);
     };
     int64_t done = 0;
+    // Several chains in binary64: the first call long enough times
+    // kTuneSweeps sweeps on each sub-sweep layout (item size, chain order)
+    // and keeps the fastest.  Every layout gives the same bits, so the probe
+    // sweeps are ordinary sweeps of the chains.
+    if (!f32(e) && e->n_chains > 1 && !e->layout_tuned && !e->profiling &&
+        n_sweeps >= kLayoutTuneMin) {
+        float best = 0.f;
+        int32_t pick = 0;
+        YM_CUDA(one_sweep());   // first launches (module loading) outside the probes
+        done += 1;
+        for (int li = 0; li < ym::kSweepLayouts; ++li) {
+            e->sweep_layout = li;
+            float t = 0.f;
+            YM_CUDA(time_on_stream(e, [&] {
+                cudaError_t err = cudaSuccess;
+                for (int64_t k = 0; k < kTuneSweeps && err == cudaSuccess; ++k) err = one_sweep();
+                return err;
+            }, &t));
+            if (li == 0 || t < best) {
+                best = t;
+                pick = li;
+            }
+            done += kTuneSweeps;
+        }
+        set_layout(e, pick);
+        e->layout_tuned = true;
+    }
     // Small chains: the first call long enough times kTuneSweeps sweeps on
     // each path and keeps the faster; the rest go to the chosen path.
-    if (resident_candidate(e)) {
-        if (e->resident_choice < 0 && n_sweeps >= 2 * kTuneSweeps) {
+    if (resident_candidate(e) && n_sweeps - done >= 2 * kTuneSweeps) {
+        if (e->resident_choice < 0) {
             float t_tiled = 0.f, t_res = 0.f;
             YM_CUDA(time_on_stream(e, [&] {
                 cudaError_t err = cudaSuccess;
@@ -530,8 +606,10 @@ int32_t ym_su3_metropolis_sweeps(ym_ensemble *e, double angle, int32_t generator
                 return ym::launch_su3_resident(e, angle, generator_mode, 1, kTuneSweeps, nullptr);
             }, &t_res));
             e->resident_choice = t_res < t_tiled ? 1 : 0;
-            done = 2 * kTuneSweeps;
+            done += 2 * kTuneSweeps;
         }
+    }
+    if (resident_candidate(e)) {
         if (e->resident_choice == 1 && done < n_sweeps) {
             YM_CUDA(ym::launch_su3_resident(e, angle, generator_mode, 1, n_sweeps - done, nullptr));
             done = n_sweeps;
@@ -805,6 +883,30 @@ int32_t ym_su3_measured_run(ym_ensemble *e, ym_ensemble *view, const ym_measured
         if (!std::isfinite(wilson[i])) return YM_ERR_NON_FINITE_OBSERVABLE;
     for (int64_t i = 0; i < run->n_blocks * e->n_chains * 2; ++i)
         if (!std::isfinite(polyakov[i])) return YM_ERR_NON_FINITE_OBSERVABLE;
+    return YM_OK;
+}
+
+int32_t ym_ensemble_set_sweep_layout(ym_ensemble *e, int32_t item_sites, int32_t by_volume) {
+    if (!e) return YM_ERR_NULL_ARGUMENT;
+    if (item_sites == 0) {                  // automatic: tune again on the next long call
+        set_layout(e, 0);
+        e->layout_tuned = false;
+        return YM_OK;
+    }
+    const int gi = item_sites == 128 ? 0 : (item_sites == 64 ? 1 : (item_sites == 32 ? 2 : -1));
+    if (gi < 0 || (by_volume != 0 && by_volume != 1)) return YM_ERR_INVALID_ARGUMENT;
+    set_layout(e, gi * 2 + by_volume);
+    e->layout_tuned = true;
+    return YM_OK;
+}
+
+int32_t ym_ensemble_get_sweep_layout(ym_ensemble *e, int32_t *item_sites, int32_t *by_volume,
+                                     int32_t *tuned) {
+    if (!e) return YM_ERR_NULL_ARGUMENT;
+    const ym::SweepLayout &l = e->layouts[e->sweep_layout];
+    if (item_sites) *item_sites = 1 << l.log2_item;
+    if (by_volume) *by_volume = l.by_volume;
+    if (tuned) *tuned = e->layout_tuned ? 1 : 0;
     return YM_OK;
 }
 

@@ -575,18 +575,22 @@ template <int MU, int K>
 __global__ void __launch_bounds__(T, YM_METRO_MIN_BLOCKS)
 k_su3_metropolis(const ChainInfo *__restrict__ chains, const Tile *__restrict__ tiles,
                  double2 *__restrict__ links, int parity, double angle, int uniform,
-                 const uint64_t *__restrict__ sweep_ptr, unsigned long long *__restrict__ accepts) {
+                 const uint64_t *__restrict__ sweep_ptr, unsigned long long *__restrict__ accepts,
+                 int log2_item) {
     __shared__ double2 sa[9][T];
     extern __shared__ __align__(16) double2 stage_mem[];
     const StageBufs bufs{reinterpret_cast<double2 (*)[T]>(stage_mem),
                          reinterpret_cast<double2 (*)[T]>(stage_mem + 9 * T),
                          reinterpret_cast<double2 (*)[T]>(stage_mem + 18 * T)};
-    const Tile tile = tiles[blockIdx.x];
-    const ChainInfo c = chains[tile.chain];
-    const int64_t t = tile.start + threadIdx.x;
+    // The CTA takes T >> log2_item work items of 2^log2_item sites each
+    // (possibly of different chains); padding items have chain < 0.
+    const Tile tile = tiles[(int64_t)blockIdx.x * (T >> log2_item) + (threadIdx.x >> log2_item)];
+    const bool live = tile.chain >= 0;
+    const ChainInfo c = chains[live ? tile.chain : 0];
+    const int64_t t = tile.start + (threadIdx.x & ((1u << log2_item) - 1u));
     const uint64_t sweep = *sweep_ptr;
     unsigned accepted = 0;
-    if (t < c.half) {
+    if (live && t < c.half) {
         const int64_t s = (int64_t)parity * c.half + t;
         const Coord x = decode_storage(c, s);
 #pragma unroll
@@ -926,12 +930,16 @@ constexpr size_t kStageBytes = 27 * T * sizeof(double2);   // three staged facto
 
 template <int K>
 static void metro_launch(ym_ensemble *e, int parity, int mu, double angle, int uniform) {
-    const dim3 grid((unsigned)e->n_half_tiles), block(T);
+    // the handle's sweep layout: work items of 2^log2 sites, chain order or
+    // by descending chain volume (all layouts give the same bits)
+    const SweepLayout &L = e->layouts[e->sweep_layout];
+    const dim3 grid((unsigned)L.ctas), block(T);
+    const Tile *items = L.d_items;
     switch (mu) {
-    case 0: k_su3_metropolis<0, K><<<grid, block, kStageBytes, e->stream>>>(e->d_chains, e->d_half_tiles, e->d_links, parity, angle, uniform, e->d_sweep, e->d_accepts); break;
-    case 1: k_su3_metropolis<1, K><<<grid, block, kStageBytes, e->stream>>>(e->d_chains, e->d_half_tiles, e->d_links, parity, angle, uniform, e->d_sweep, e->d_accepts); break;
-    case 2: k_su3_metropolis<2, K><<<grid, block, kStageBytes, e->stream>>>(e->d_chains, e->d_half_tiles, e->d_links, parity, angle, uniform, e->d_sweep, e->d_accepts); break;
-    default: k_su3_metropolis<3, K><<<grid, block, kStageBytes, e->stream>>>(e->d_chains, e->d_half_tiles, e->d_links, parity, angle, uniform, e->d_sweep, e->d_accepts); break;
+    case 0: k_su3_metropolis<0, K><<<grid, block, kStageBytes, e->stream>>>(e->d_chains, items, e->d_links, parity, angle, uniform, e->d_sweep, e->d_accepts, L.log2_item); break;
+    case 1: k_su3_metropolis<1, K><<<grid, block, kStageBytes, e->stream>>>(e->d_chains, items, e->d_links, parity, angle, uniform, e->d_sweep, e->d_accepts, L.log2_item); break;
+    case 2: k_su3_metropolis<2, K><<<grid, block, kStageBytes, e->stream>>>(e->d_chains, items, e->d_links, parity, angle, uniform, e->d_sweep, e->d_accepts, L.log2_item); break;
+    default: k_su3_metropolis<3, K><<<grid, block, kStageBytes, e->stream>>>(e->d_chains, items, e->d_links, parity, angle, uniform, e->d_sweep, e->d_accepts, L.log2_item); break;
     }
 }
 

@@ -22,6 +22,18 @@ inline int64_t lp_reduce_groups(int64_t tiles) { return (tiles + 63) / 64; }
 // failure as the calling thread's ym_last_cuda_error (capi.cu).
 int32_t record_cuda_status(cudaError_t err);
 
+// One work layout of the SU(3) FP64 sub-sweep: a table of work items of
+// 2^log2_item sites (a 128-thread CTA takes 128 >> log2_item of them, so
+// items of different chains can share a CTA), padded with chain = -1 items
+// to whole CTAs.
+struct SweepLayout {
+    Tile *d_items = nullptr;
+    int64_t ctas = 0;
+    int32_t log2_item = 7;
+    int32_t by_volume = 0;     // items of the largest chains first
+};
+constexpr int kSweepLayouts = 6;   // item sizes 128, 64, 32 x (chain order, by volume)
+
 }  // namespace ym
 
 struct ym_ensemble {
@@ -92,6 +104,12 @@ struct ym_ensemble {
     // Small-chain path choice: -1 not yet measured, 0 tiled launches, 1 the
     // chain-resident kernel (picked by timing both on the first sweeps).
     int32_t resident_choice = -1;
+    // Sub-sweep layouts of the SU(3) FP64 sweep and the one in use (picked
+    // by timing each on the first long sweep call of a handle with several
+    // chains, or set by the caller).
+    ym::SweepLayout layouts[ym::kSweepLayouts];
+    int32_t sweep_layout = 0;
+    bool layout_tuned = false;
     // Half widths above the reference's 1.0 admitted (two-row handles only).
     bool angle_cap_lifted = false;
     // Captured block of the loop-measurement cadence (ym_su3_measured_run):

@@ -175,6 +175,19 @@ class Ensemble:
               "su3_measured_run")
         return plaq, wil, pol[..., 0] + 1j * pol[..., 1]
 
+    @property
+    def sweep_layout(self) -> dict:
+        """The SU(3) FP64 sub-sweep's work layout: item size, order, tuned."""
+        n, v, t = C.c_int32(), C.c_int32(), C.c_int32()
+        check(lib().ym_ensemble_get_sweep_layout(self._h, C.byref(n), C.byref(v), C.byref(t)),
+              "get_sweep_layout")
+        return {"item_sites": n.value, "by_volume": bool(v.value), "tuned": bool(t.value)}
+
+    def set_sweep_layout(self, item_sites: int = 0, by_volume: bool = False) -> None:
+        """Force a layout (item_sites 128/64/32) or ask for tuning (0)."""
+        check(lib().ym_ensemble_set_sweep_layout(self._h, int(item_sites), int(by_volume)),
+              "set_sweep_layout")
+
     def lift_angle_cap(self, lift: bool = True) -> None:
         """Admit half widths up to 2.5 on a two-row handle (past the
         reference's 1.0), for plain Metropolis at a learned scale."""

@@ -215,6 +215,8 @@ class GlueballPipelineResult:
     sweep_seconds: float = 0.0
     measure_seconds: float = 0.0
     link_updates: int = 0
+    sweep_layout: dict = field(default_factory=dict)   # the handle tuner's choice
+    sweep_path: str = ""
 
 
 def _blockable(e) -> bool:
@@ -254,6 +256,8 @@ def scalar_glueball_pipeline(groups: Sequence[Tuple[int, Sequence[int]]] = ((128
             ens.metropolis_sweeps(proposal_angle, thermalization)
             ens.synchronize()
             res.sweep_seconds += time.perf_counter() - t0
+            res.sweep_layout = ens.sweep_layout
+            res.sweep_path = ens.sweep_path
             for _ in range(measurements):
                 t0 = time.perf_counter()
                 ens.metropolis_sweeps(proposal_angle, sweeps_between_measurements)
