@@ -370,6 +370,35 @@ int32_t ym_su3_spatial_stout_smear(ym_ensemble *src, ym_ensemble *dst, double rh
  * blocked extents (N0/2, N1/2, N2/2, N3) of every src chain. */
 int32_t ym_su3_spatial_stride2_block(ym_ensemble *src, ym_ensemble *dst);
 
+/* One measurement of the scalar-glueball production cadence
+ * (glueball_scalar_production.rs:257-381, per retained configuration): the
+ * links of `ens` copied into `smeared` (same extents), then for each stout
+ * level count in `levels` (ascending; 0 allowed) the levels smeared in place
+ * continuing from the previous count (sequential levels, so the same links
+ * as smearing from scratch; spatial_stout_smear glueball_smearing.rs:257),
+ * scalar_a1pp_operator_basis of every chain (glueball_operators.rs:93-160),
+ * and for every blocked group g the chains first_chain[g].. of `smeared`
+ * copied into fine[g], spatial_stride2_block into coarse[g]
+ * (glueball_blocking.rs:105-136) and its operator basis.  The whole
+ * measurement is one captured CUDA graph, replayed on later calls with the
+ * same plan and handles, with a single synchronisation at the end.
+ *   plaquette, rectangle          [n_levels][slices of smeared]
+ *   blocked_plaquette, _rectangle [n_levels][slices of coarse[0], coarse[1], ...]
+ * (slices: every chain's time slices t = 0..N3-1, chain by chain, as
+ * ym_su3_scalar_operator_basis returns them). */
+typedef struct {
+    double rho;                      /* (0, 0.25] */
+    int32_t n_levels;
+    const int64_t *levels;
+    int32_t n_blocked;
+    ym_ensemble *const *fine;        /* n_blocked handles */
+    ym_ensemble *const *coarse;      /* n_blocked handles of the blocked extents */
+    const int64_t *first_chain;      /* n_blocked */
+} ym_glueball_plan;
+int32_t ym_su3_glueball_measure(ym_ensemble *ens, ym_ensemble *smeared, const ym_glueball_plan *plan,
+                                double *plaquette, double *rectangle, double *blocked_plaquette,
+                                double *blocked_rectangle);
+
 /* ---- two-row binary32 storage (YM_PREC_F32_TWO_ROW, no reference
  * counterpart: the reference stores 18 doubles per link) ----
  * Gram-Schmidt of every link's two stored rows in binary64, rounded back;

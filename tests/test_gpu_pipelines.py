@@ -137,3 +137,46 @@ def test_sweep_layouts_give_the_same_bits_and_the_tuner_picks_one(oracle):
         for c in range(len(exts)):
             assert np.array_equal(a.download(c), b.download(c))
         assert np.array_equal(a.accounting()[1], b.accounting()[1])
+
+
+def test_glueball_measurement_graph_equals_separate_calls(oracle):
+    """ym_su3_glueball_measure (copy, incremental stout levels, operator
+    bases, group blocking, one captured graph) equals the same measurement
+    made call by call, bit for bit, on two calls in a row (the second replays
+    the graph)."""
+    import ymgpu
+    from ymgpu import glueball as G
+    exts = [[4, 4, 4, 6]] * 2 + [[6, 6, 6, 4]] * 2
+    with ymgpu.Ensemble(exts, 5.7, [1, 2, 3, 4]) as ens, ymgpu.Ensemble(exts, 5.7, [1, 2, 3, 4]) as sm:
+        ens.hot_start()
+        ens.metropolis_sweeps(1.0, 6, "uniform")
+        fine = sm.subset([2, 3])
+        coarse = fine.like([G.blocked_extents(e) for e in fine.extents])
+        ref_sm = ens.like()
+        ref_fine = fine.like()
+        ref_coarse = coarse.like()
+        try:
+            for _ in range(2):
+                got = ens.glueball_measure(sm, [0, 2, 3], 0.1, [(fine, coarse, 2)])
+                ens.copy_to(ref_sm)
+                done, want_p, want_r, want_bp, want_br = 0, [], [], [], []
+                for lv in (0, 2, 3):
+                    if lv > done:
+                        ref_sm.stout_smear_into(ref_sm, 0.1, lv - done, lift_level_cap=True)
+                        done = lv
+                    basis = ref_sm.scalar_operator_basis()
+                    want_p.append(np.concatenate([b[0] for b in basis]))
+                    want_r.append(np.concatenate([b[1] for b in basis]))
+                    ref_sm.copy_subset_to([2, 3], ref_fine)
+                    ref_fine.block_into(ref_coarse)
+                    cb = ref_coarse.scalar_operator_basis()
+                    want_bp.append(np.concatenate([b[0] for b in cb]))
+                    want_br.append(np.concatenate([b[1] for b in cb]))
+                assert np.array_equal(got[0], np.array(want_p))
+                assert np.array_equal(got[1], np.array(want_r))
+                assert np.array_equal(got[2], np.array(want_bp))
+                assert np.array_equal(got[3], np.array(want_br))
+                ens.metropolis_sweeps(0.35, 2, "ordered")
+        finally:
+            for h in (fine, coarse, ref_sm, ref_fine, ref_coarse):
+                h.close()

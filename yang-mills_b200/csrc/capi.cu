@@ -58,6 +58,8 @@ void free_all(ym_ensemble *e) {
     if (e->sweep_graph) cudaGraphExecDestroy(e->sweep_graph);
     if (e->measure_graph) cudaGraphExecDestroy(e->measure_graph);
     if (e->run_graph) cudaGraphExecDestroy(e->run_graph);
+    if (e->glueball_graph) cudaGraphExecDestroy(e->glueball_graph);
+    if (e->d_gb_series) cudaFree(e->d_gb_series);
     if (e->d_series) cudaFree(e->d_series);
     if (e->d_wilson_series) cudaFree(e->d_wilson_series);
     if (e->d_poly_series) cudaFree(e->d_poly_series);
@@ -1244,6 +1246,192 @@ int32_t ym_su3_spatial_stride2_block(ym_ensemble *src, ym_ensemble *dst) {
     YM_CUDA(cudaStreamSynchronize(src->stream));
     YM_CUDA(ym::launch_block(src, dst));
     return take_device_error(dst);
+}
+
+int32_t ym_su3_glueball_measure(ym_ensemble *ens, ym_ensemble *sm, const ym_glueball_plan *plan,
+                                double *plaquette, double *rectangle, double *blocked_plaquette,
+                                double *blocked_rectangle) {
+    if (!ens || !sm || !plan || !plaquette || !rectangle) return YM_ERR_NULL_ARGUMENT;
+    if (plan->n_levels < 1 || !plan->levels || plan->n_blocked < 0) return YM_ERR_INVALID_ARGUMENT;
+    if (plan->n_blocked > 0 && (!plan->fine || !plan->coarse || !plan->first_chain ||
+                                !blocked_plaquette || !blocked_rectangle))
+        return YM_ERR_NULL_ARGUMENT;
+    { const int32_t g__ = require_su3_f64(ens); if (g__) return g__; }
+    if (!same_geometry(ens, sm)) return YM_ERR_LATTICE_EXTENTS_MISMATCH;
+    // validate_parameters (glueball_smearing.rs:83-108) and the operator
+    // basis' spatial check (glueball_operators.rs:72-91)
+    if (!std::isfinite(plan->rho)) return YM_ERR_NON_FINITE_RHO;
+    if (plan->rho <= 0.0 || plan->rho > 0.25) return YM_ERR_RHO_OUT_OF_RANGE;
+    for (int32_t i = 0; i < plan->n_levels; ++i)
+        if (plan->levels[i] < 0 || (i && plan->levels[i] < plan->levels[i - 1])) return YM_ERR_INVALID_ARGUMENT;
+    int32_t st = require_cubic_spatial(sm, 3);
+    if (st) return st;
+    int64_t blocked_slices = 0;
+    for (int32_t g = 0; g < plan->n_blocked; ++g) {
+        ym_ensemble *f = plan->fine[g], *c = plan->coarse[g];
+        if (!f || !c) return YM_ERR_NULL_ARGUMENT;
+        { const int32_t g__ = require_su3_f64(f); if (g__) return g__; }
+        { const int32_t g__ = require_su3_f64(c); if (g__) return g__; }
+        const int64_t first = plan->first_chain[g];
+        if (first < 0 || first > sm->n_chains - f->n_chains || f->device != sm->device ||
+            c->device != sm->device || c->n_chains != f->n_chains)
+            return YM_ERR_INVALID_ARGUMENT;
+        for (int64_t k = 0; k < f->n_chains; ++k) {
+            const ChainInfo &a = sm->chains[first + k], &b = f->chains[k], &q = c->chains[k];
+            for (int d = 0; d < 4; ++d)
+                if (a.n[d] != b.n[d]) return YM_ERR_LATTICE_EXTENTS_MISMATCH;
+            // validate_geometry (glueball_blocking.rs:71-83)
+            if (b.n[0] != b.n[1] || b.n[1] != b.n[2]) return YM_ERR_SPATIAL_EXTENTS_NOT_CUBIC;
+            if (b.n[0] < 6) return YM_ERR_SPATIAL_EXTENT_TOO_SMALL;
+            if (b.n[0] % 2 != 0) return YM_ERR_SPATIAL_EXTENT_NOT_EVEN;
+            if (q.n[0] * 2 != b.n[0] || q.n[1] * 2 != b.n[1] || q.n[2] * 2 != b.n[2] || q.n[3] != b.n[3])
+                return YM_ERR_LATTICE_EXTENTS_MISMATCH;
+        }
+        if ((st = require_cubic_spatial(c, 3))) return st;
+    }
+    if ((st = set_device(sm))) return st;
+    // scratch of every handle, made before any capture
+    YM_CUDA(ensure_obs_scratch(sm));
+    if (!sm->d_links_tmp) YM_CUDA(dalloc(&sm->d_links_tmp, (size_t)sm->total_elems));
+    for (int32_t g = 0; g < plan->n_blocked; ++g) {
+        YM_CUDA(ensure_obs_scratch(plan->coarse[g]));
+        blocked_slices += plan->coarse[g]->n_slices;
+    }
+    const int64_t per_level = 2 * (sm->n_slices + blocked_slices);
+    const int64_t need = per_level * plan->n_levels;
+    // what a captured graph was made for: levels, handles and their buffers
+    std::vector<int64_t> key;
+    key.push_back(plan->n_levels);
+    for (int32_t i = 0; i < plan->n_levels; ++i) key.push_back(plan->levels[i]);
+    key.push_back((int64_t)(uintptr_t)ens->d_links);
+    key.push_back((int64_t)(uintptr_t)sm->d_links);
+    for (int32_t g = 0; g < plan->n_blocked; ++g) {
+        key.push_back(plan->first_chain[g]);
+        key.push_back((int64_t)(uintptr_t)plan->fine[g]->d_links);
+        key.push_back((int64_t)(uintptr_t)plan->coarse[g]->d_links);
+        key.push_back((int64_t)(uintptr_t)plan->coarse[g]->d_slice_plaq);
+    }
+    if (sm->gb_series_capacity < need) {
+        if (sm->glueball_graph) cudaGraphExecDestroy(sm->glueball_graph);
+        sm->glueball_graph = nullptr;
+        if (sm->d_gb_series) cudaFree(sm->d_gb_series);
+        sm->d_gb_series = nullptr;
+        sm->gb_series_capacity = 0;
+        YM_CUDA(dalloc(&sm->d_gb_series, (size_t)need));
+        sm->gb_series_capacity = need;
+    }
+    // ens's own work (its sweeps) is done before the copy reads its links
+    YM_CUDA(cudaStreamSynchronize(ens->stream));
+    for (int32_t g = 0; g < plan->n_blocked; ++g) {
+        YM_CUDA(cudaStreamSynchronize(plan->fine[g]->stream));
+        YM_CUDA(cudaStreamSynchronize(plan->coarse[g]->stream));
+    }
+    auto measure = [&]() -> cudaError_t {
+        cudaStream_t s0 = sm->stream;
+        cudaError_t err = cudaMemcpyAsync(sm->d_links, ens->d_links, (size_t)sm->total_elems * sizeof(double2),
+                                          cudaMemcpyDeviceToDevice, s0);
+        int64_t done = 0;
+        for (int32_t i = 0; i < plan->n_levels && err == cudaSuccess; ++i) {
+            // levels continue from the previous count, in place (the
+            // ping-pong of ym_su3_spatial_stout_smear with src == dst)
+            const int64_t n = plan->levels[i] - done;
+            if (n > 0) {
+                const double2 *in = sm->d_links;
+                if (n % 2 == 1) {
+                    err = cudaMemcpyAsync(sm->d_links_tmp, sm->d_links, (size_t)sm->total_elems * sizeof(double2),
+                                          cudaMemcpyDeviceToDevice, s0);
+                    in = sm->d_links_tmp;
+                }
+                for (int64_t k = 1; k <= n && err == cudaSuccess; ++k) {
+                    double2 *out = ((n - k) % 2 == 0) ? sm->d_links : sm->d_links_tmp;
+                    err = ym::launch_stout_level(sm, in, out, plan->rho);
+                    in = out;
+                }
+                done = plan->levels[i];
+            }
+            double *row = sm->d_gb_series + per_level * i;
+            if (err == cudaSuccess)
+                err = ym::launch_operator_basis(sm, sm->d_site_vals, sm->d_slice_chain, sm->d_slice_t,
+                                                sm->n_slices, sm->d_slice_plaq, sm->d_slice_rect);
+            if (err == cudaSuccess)
+                err = cudaMemcpyAsync(row, sm->d_slice_plaq, (size_t)sm->n_slices * sizeof(double),
+                                      cudaMemcpyDeviceToDevice, s0);
+            if (err == cudaSuccess)
+                err = cudaMemcpyAsync(row + sm->n_slices, sm->d_slice_rect, (size_t)sm->n_slices * sizeof(double),
+                                      cudaMemcpyDeviceToDevice, s0);
+            double *brow = row + 2 * sm->n_slices;
+            for (int32_t g = 0; g < plan->n_blocked && err == cudaSuccess; ++g) {
+                ym_ensemble *f = plan->fine[g], *c = plan->coarse[g];
+                const ChainInfo &a = sm->chains[plan->first_chain[g]];
+                const ChainInfo &z = sm->chains[plan->first_chain[g] + f->n_chains - 1];
+                const size_t bytes = (size_t)(z.offset - a.offset + z.volume * 36) * sizeof(double2);
+                err = cudaMemcpyAsync(f->d_links, sm->d_links + a.offset, bytes, cudaMemcpyDeviceToDevice, s0);
+                if (err == cudaSuccess) err = ym::launch_block(f, c);
+                if (err == cudaSuccess)
+                    err = ym::launch_operator_basis(c, c->d_site_vals, c->d_slice_chain, c->d_slice_t, c->n_slices,
+                                                    c->d_slice_plaq, c->d_slice_rect);
+                if (err == cudaSuccess)
+                    err = cudaMemcpyAsync(brow, c->d_slice_plaq, (size_t)c->n_slices * sizeof(double),
+                                          cudaMemcpyDeviceToDevice, s0);
+                if (err == cudaSuccess)
+                    err = cudaMemcpyAsync(brow + blocked_slices, c->d_slice_rect, (size_t)c->n_slices * sizeof(double),
+                                          cudaMemcpyDeviceToDevice, s0);
+                brow += c->n_slices;
+            }
+        }
+        return err;
+    };
+    if (!sm->glueball_graph || sm->glueball_key != key || sm->glueball_rho != plan->rho) {
+        if (sm->glueball_graph) cudaGraphExecDestroy(sm->glueball_graph);
+        sm->glueball_graph = nullptr;
+        // the blocked handles' launches join the capture on sm's stream
+        std::vector<cudaStream_t> saved;
+        for (int32_t g = 0; g < plan->n_blocked; ++g) {
+            saved.push_back(plan->fine[g]->stream);
+            saved.push_back(plan->coarse[g]->stream);
+            plan->fine[g]->stream = sm->stream;
+            plan->coarse[g]->stream = sm->stream;
+        }
+        cudaGraph_t graph = nullptr;
+        cudaError_t err = cudaStreamBeginCapture(sm->stream, cudaStreamCaptureModeThreadLocal);
+        if (err == cudaSuccess) {
+            err = measure();
+            const cudaError_t end = cudaStreamEndCapture(sm->stream, &graph);
+            if (err == cudaSuccess) err = end;
+        }
+        for (int32_t g = 0; g < plan->n_blocked; ++g) {
+            plan->fine[g]->stream = saved[(size_t)2 * g];
+            plan->coarse[g]->stream = saved[(size_t)2 * g + 1];
+        }
+        if (err == cudaSuccess) err = cudaGraphInstantiate(&sm->glueball_graph, graph, 0);
+        if (graph) cudaGraphDestroy(graph);
+        YM_CUDA(err);
+        sm->glueball_key = key;
+        sm->glueball_rho = plan->rho;
+    }
+    YM_CUDA(cudaGraphLaunch(sm->glueball_graph, sm->stream));
+    std::vector<double> host((size_t)need);
+    YM_CUDA(cudaMemcpyAsync(host.data(), sm->d_gb_series, (size_t)need * sizeof(double), cudaMemcpyDeviceToHost,
+                            sm->stream));
+    YM_CUDA(cudaStreamSynchronize(sm->stream));
+    // gates of the kernels that ran (stout: sm's flag, blocking: each coarse flag)
+    if ((st = take_device_error(sm))) return st;
+    for (int32_t g = 0; g < plan->n_blocked; ++g)
+        if ((st = take_device_error(plan->coarse[g]))) return st;
+    for (int32_t i = 0; i < plan->n_levels; ++i) {
+        const double *row = host.data() + per_level * i;
+        for (int64_t k = 0; k < sm->n_slices; ++k) {
+            plaquette[i * sm->n_slices + k] = row[k];
+            rectangle[i * sm->n_slices + k] = row[sm->n_slices + k];
+        }
+        for (int64_t k = 0; k < blocked_slices; ++k) {
+            blocked_plaquette[i * blocked_slices + k] = row[2 * sm->n_slices + k];
+            blocked_rectangle[i * blocked_slices + k] = row[2 * sm->n_slices + blocked_slices + k];
+        }
+    }
+    for (int64_t k = 0; k < need; ++k)
+        if (!std::isfinite(host[(size_t)k])) return YM_ERR_NON_FINITE_OBSERVABLE;
+    return YM_OK;
 }
 
 int32_t ym_su3_reunitarize(ym_ensemble *e) {

@@ -20,85 +20,15 @@ namespace ym {
 // ------------------------------------------------------------ reductions
 
 // Sum of the six plaquette values (1/3) Re Tr P of each site, site order
-// (mu, nu) = (0,1),(0,2),(0,3),(1,2),(1,3),(2,3), per tile.  The arithmetic
-// is site_plaquette_sum's, operation for operation (so the chain-resident
-// path's plaquettes stay bitwise equal); the two neighbour links of each
-// plane, U_nu(x+mu) and U_mu(x+nu), are copied global -> shared by
-// L1-allocating cp.async one plane ahead, so a plane's loads overlap the
-// previous plane's products instead of each plane waiting on its own.
-constexpr int kPlaqStageEntries = 2 * 2 * 9;   // 2 buffers x 2 links x 9 entries
-
-__device__ __forceinline__ void plaq_stage(double2 *buf, const double2 *links, const ChainInfo &c,
-                                           int64_t s1, int d1, int64_t s2, int d2) {
-    const double2 *p1 = links + c.offset + (int64_t)(d1 * 9) * c.volume + s1;
-    const double2 *p2 = links + c.offset + (int64_t)(d2 * 9) * c.volume + s2;
-#pragma unroll
-    for (int e = 0; e < 9; ++e) {
-        cp_async16_ca(buf + (size_t)e * kSiteThreads + threadIdx.x, p1 + (int64_t)e * c.volume);
-        cp_async16_ca(buf + (size_t)(9 + e) * kSiteThreads + threadIdx.x, p2 + (int64_t)e * c.volume);
-    }
-    cp_async_commit();
-}
-
-__device__ __forceinline__ m3 plaq_staged(const double2 *buf, int which) {
-    m3 o;
-#pragma unroll
-    for (int e = 0; e < 9; ++e) {
-        const double2 v = buf[(size_t)(9 * which + e) * kSiteThreads + threadIdx.x];
-        o.e[e / 3][e % 3] = cmake(v.x, v.y);
-    }
-    return o;
-}
-
-// Storage slots of plane (mu, nu)'s neighbour sites x+mu and x+nu.
-__device__ __forceinline__ void plaq_plane_sites(const ChainInfo &c, const Coord &x, int mu, int nu,
-                                                 int64_t &s1, int64_t &s2) {
-    const Nb pm = step_any(c, x.x, x.lex, x.par, mu, +1);
-    const Nb pn = step_any(c, x.x, x.lex, x.par, nu, +1);
-    s1 = storage_index(c, pm.lex, pm.par);
-    s2 = storage_index(c, pn.lex, pn.par);
-}
-
-// plane k -> (mu, nu): (0,1),(0,2),(0,3),(1,2),(1,3),(2,3)
-__device__ __forceinline__ int plane_mu(int k) { return (k >= 3 ? 1 : 0) + (k >= 5 ? 1 : 0); }
-__device__ __forceinline__ int plane_nu(int k) { return k < 3 ? k + 1 : (k < 5 ? k - 1 : 3); }
-
-__global__ void __launch_bounds__(kSiteThreads, 3)
+// (mu, nu) = (0,1),(0,2),(0,3),(1,2),(1,3),(2,3), per tile.
+__global__ void __launch_bounds__(kSiteThreads)
 k_su3_plaquette(const ChainInfo *__restrict__ chains, const Tile *__restrict__ tiles,
                 const double2 *__restrict__ links, double *__restrict__ partial) {
-    extern __shared__ __align__(16) double2 plaq_buf[];
     const Tile tile = tiles[blockIdx.x];
     const ChainInfo c = chains[tile.chain];
     const int64_t s = tile.start + threadIdx.x;
     double v = 0.0;
-    if (s < c.volume) {
-        const Coord x = decode_storage(c, s);
-        int64_t s1, s2;
-        plaq_plane_sites(c, x, 0, 1, s1, s2);
-        plaq_stage(plaq_buf, links, c, s1, 1, s2, 0);
-        m3 umu;
-        bool first = true;
-#pragma unroll 1
-        for (int k = 0; k < 6; ++k) {
-            const int mu = plane_mu(k), nu = plane_nu(k);
-            const double2 *cur = plaq_buf + (size_t)(k & 1) * 18 * kSiteThreads;
-            if (k < 5) {
-                int64_t n1, n2;
-                plaq_plane_sites(c, x, plane_mu(k + 1), plane_nu(k + 1), n1, n2);
-                plaq_stage(plaq_buf + (size_t)((k + 1) & 1) * 18 * kSiteThreads, links, c, n1,
-                           plane_nu(k + 1), n2, plane_mu(k + 1));
-                cp_async_wait_one();
-            } else {
-                cp_async_wait_all();
-            }
-            if (k == 0 || k == 3 || k == 5) umu = load_su3(links, c, s, mu);
-            m3 p = mul_fma(umu, plaq_staged(cur, 0));
-            p = mul_adj_fma(p, plaq_staged(cur, 1));
-            const double val = retrace_mul_adj(p, load_su3(links, c, s, nu)) / 3.0;
-            v = first ? val : v + val;
-            first = false;
-        }
-    }
+    if (s < c.volume) v = site_plaquette_sum<false>(links, c, s);
     v = block_reduce<false>(v);
     if (threadIdx.x == 0) partial[blockIdx.x] = v;
 }
@@ -404,20 +334,7 @@ cudaError_t launch_chain_reduce(ym_ensemble *e, const double *partial, double *o
 }
 
 cudaError_t launch_su3_plaquette(ym_ensemble *e) {
-    constexpr size_t smem = (size_t)kPlaqStageEntries * kSiteThreads * sizeof(double2);
-    static thread_local int configured_device = -1;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (configured_device != dev) {
-        cudaError_t err = cudaFuncSetAttribute(k_su3_plaquette, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               (int)smem);
-        if (err == cudaSuccess)
-            err = cudaFuncSetAttribute(k_su3_plaquette, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                       cudaSharedmemCarveoutMaxShared);
-        if (err != cudaSuccess) return err;
-        configured_device = dev;
-    }
-    k_su3_plaquette<<<(unsigned)e->n_site_tiles, kSiteThreads, smem, e->stream>>>(
+    k_su3_plaquette<<<(unsigned)e->n_site_tiles, kSiteThreads, 0, e->stream>>>(
         e->d_chains, e->d_site_tiles, e->d_links, e->d_partial);
     k_chain_reduce<<<(unsigned)e->n_chains, 256, 0, e->stream>>>(
         e->d_partial, e->d_site_tile_first, e->d_chains, e->d_result, 0, 6.0);

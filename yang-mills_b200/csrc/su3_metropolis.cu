@@ -421,11 +421,11 @@ __device__ __forceinline__ void lambda8_fixed(double theta, cplx &e1, cplx &e2) 
 }
 
 struct BlockPre {
-    double c, s, unif, nlog;
+    double c, s, unif;
 };
 struct DiagPre {
     cplx e1, e2;
-    double unif, nlog;
+    double unif;
 };
 
 template <int K>
@@ -433,9 +433,6 @@ __device__ __forceinline__ BlockPre pre_block(uint64_t key, int h, double angle)
     BlockPre p;
     taylor_fixed<K>(0.5 * grid_angle(splitmix_at(key, (uint64_t)(2 * h)), angle), p.c, p.s);
     p.unif = unit_from(splitmix_at(key, (uint64_t)(2 * h + 1)));
-#ifdef YM_METRO_LOG_DECISION
-    p.nlog = -log(p.unif);
-#endif
     return p;
 }
 
@@ -444,29 +441,7 @@ __device__ __forceinline__ DiagPre pre_diag(uint64_t key, int h, double angle) {
     DiagPre p;
     lambda8_fixed<K>(grid_angle(splitmix_at(key, (uint64_t)(2 * h)), angle), p.e1, p.e2);
     p.unif = unit_from(splitmix_at(key, (uint64_t)(2 * h + 1)));
-#ifdef YM_METRO_LOG_DECISION
-    p.nlog = -log(p.unif);
-#endif
     return p;
-}
-
-// u < exp(-m).  With YM_METRO_LOG_DECISION it is decided from L = -log(u),
-// computed off the link's dependency chain: m <= L - eps accepts and
-// m >= L + eps rejects exactly as the test itself would (log and exp are
-// each within an ulp and |L| <= 37, so the 1e-12 margin keeps exp(-m) and u
-// apart by a factor of at least 1 + 1e-12); only inside the band
-// (probability ~1e-12 per hit) is exp evaluated.
-__device__ __forceinline__ bool decide(double m, double unif, double nlog) {
-#ifdef YM_METRO_LOG_DECISION
-    constexpr double kBand = 1e-12;
-    bool acc = m <= nlog - kBand;
-    const bool rej = m >= nlog + kBand;
-    if (!acc && !rej) acc = unif < exp(-m);
-    return acc;
-#else
-    (void)nlog;
-    return unif < exp(-m);
-#endif
 }
 
 // hit_block for a compile-time generator, decision by selects.
@@ -498,7 +473,7 @@ __device__ __forceinline__ void hit_block_sel(m3 &u, const double2 (*sa)[T], dou
     q[I1] = retr_row_fma(n1, col1);
     const double new_tr = (q[0] + q[1]) + q[2];
     const double m = fmax(beta3 * (old_tr - new_tr), 0.0);
-    const bool acc = decide(m, p.unif, p.nlog);
+    const bool acc = p.unif < exp(-m);
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         u.e[I0][k] = acc ? n0[k] : u.e[I0][k];
@@ -525,7 +500,7 @@ __device__ __forceinline__ void hit_diag_sel(m3 &u, const double2 (*sa)[T], doub
     }
     const double new_tr = (q[0] + q[1]) + q[2];
     const double m = fmax(beta3 * (old_tr - new_tr), 0.0);
-    const bool acc = decide(m, p.unif, p.nlog);
+    const bool acc = p.unif < exp(-m);
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
 #pragma unroll
@@ -600,7 +575,7 @@ k_su3_metropolis(const ChainInfo *__restrict__ chains, const Tile *__restrict__ 
         cp_async_wait_all();
         m3 u = staged_link(bufs.l1);
         const uint64_t key = link_key(c.seed, sweep, x.lex, MU);
-        accepted = K ? visit_ordered<K>(u, sa, c.beta / 3.0, angle, key)
+        accepted = K ? visit_ordered<K ? K : 13>(u, sa, c.beta / 3.0, angle, key)
                      : visit(u, sa, c.beta / 3.0, angle, key, uniform);
         store_su3(links, c, s, MU, u);
     }

@@ -125,6 +125,14 @@ struct ym_ensemble {
     double *d_poly_series = nullptr;       // [block][chain][2]
     int64_t loop_capacity = 0;             // rows
     uint64_t *d_loop_row = nullptr;
+    // Captured glueball measurement (ym_su3_glueball_measure), kept on the
+    // smeared handle: the graph, what it was captured for, and its outputs
+    // [level][slice] for this handle and for the blocked handles.
+    cudaGraphExec_t glueball_graph = nullptr;
+    std::vector<int64_t> glueball_key;
+    double glueball_rho = 0.0;
+    double *d_gb_series = nullptr;
+    int64_t gb_series_capacity = 0;        // doubles
     double *d_series = nullptr;            // [measurement][chain]
     int64_t series_capacity = 0;           // rows
     uint64_t *d_series_row = nullptr;

@@ -28,6 +28,11 @@ class MeasuredRun(C.Structure):
                 ("n_blocks", i64), ("sweeps_per_block", i64), ("rmax", i32), ("tmax", i32)]
 
 
+class GlueballPlan(C.Structure):
+    _fields_ = [("rho", f64), ("n_levels", i32), ("levels", P(i64)), ("n_blocked", i32),
+                ("fine", P(VP)), ("coarse", P(VP)), ("first_chain", P(i64))]
+
+
 # name -> (argtypes); every function returns int32 ym_status
 SIGNATURES = {
     "ym_last_cuda_error": [],
@@ -83,6 +88,7 @@ SIGNATURES = {
     "ym_ensemble_copy_chains": [VP, i64, VP, i64, i64],
     "ym_su3_spatial_stout_smear": [VP, VP, f64, i64, i32],
     "ym_su3_spatial_stride2_block": [VP, VP],
+    "ym_su3_glueball_measure": [VP, VP, P(GlueballPlan), P(f64), P(f64), P(f64), P(f64)],
     "ym_periodic_connected_estimator": [P(f64), i64, i64, P(f64), P(f64), P(f64)],
     "ym_connected_from_samples": [P(f64), i64, i64, i64, P(f64)],
     "ym_jackknife_replicas": [P(f64), i64, i64, P(f64)],

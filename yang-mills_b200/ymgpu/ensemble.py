@@ -14,7 +14,7 @@ from typing import Sequence
 
 import numpy as np
 
-from ._lib import EnsembleDesc, MeasuredRun, lib
+from ._lib import EnsembleDesc, GlueballPlan, MeasuredRun, lib
 from .errors import check
 
 SU2, SU3 = 2, 3
@@ -453,6 +453,30 @@ class Ensemble:
                          lift_level_cap: bool = False) -> None:
         check(lib().ym_su3_spatial_stout_smear(self._h, dst.handle, float(rho), int(levels),
                                                int(lift_level_cap)), "spatial_stout_smear")
+
+    def glueball_measure(self, smeared: "Ensemble", levels, rho: float = 0.1, blocked=()):
+        """One glueball measurement as one captured graph (ym_su3_glueball_measure):
+        this handle's links smeared in place in `smeared` through the
+        ascending level counts, the A1++ operator basis after each count, and
+        for each (fine, coarse, first_chain) in `blocked` the chains
+        first_chain.. of `smeared` blocked into `coarse` and measured.
+        Returns (plaquette, rectangle, blocked_plaquette, blocked_rectangle),
+        each [level, slice]."""
+        lv = np.ascontiguousarray(np.asarray(levels, dtype=np.int64))
+        blocked = list(blocked)
+        fine = (C.c_void_p * max(1, len(blocked)))(*[b[0].handle.value for b in blocked])
+        coarse = (C.c_void_p * max(1, len(blocked)))(*[b[1].handle.value for b in blocked])
+        first = np.ascontiguousarray(np.asarray([b[2] for b in blocked] or [0], dtype=np.int64))
+        plan = GlueballPlan(float(rho), len(lv), _i64p(lv), len(blocked), fine, coarse, _i64p(first))
+        n_sl = sum(e[3] for e in smeared.extents)
+        n_bl = sum(sum(e[3] for e in b[1].extents) for b in blocked)
+        p = np.zeros((len(lv), n_sl), np.float64)
+        r = np.zeros((len(lv), n_sl), np.float64)
+        bp = np.zeros((len(lv), max(n_bl, 1)), np.float64)
+        br = np.zeros((len(lv), max(n_bl, 1)), np.float64)
+        check(lib().ym_su3_glueball_measure(self._h, smeared.handle, C.byref(plan), _f64p(p), _f64p(r),
+                                            _f64p(bp), _f64p(br)), "glueball_measure")
+        return p, r, bp[:, :n_bl], br[:, :n_bl]
 
     def block_into(self, dst: "Ensemble") -> None:
         check(lib().ym_su3_spatial_stride2_block(self._h, dst.handle), "spatial_stride2_block")

@@ -251,6 +251,14 @@ def scalar_glueball_pipeline(groups: Sequence[Tuple[int, Sequence[int]]] = ((128
             if _blockable(groups[gi][1]):
                 subs[gi] = sm.subset(chains)
                 coarse[gi] = subs[gi].like([G.blocked_extents(e) for e in subs[gi].extents])
+        blocked_groups = sorted(subs)
+        # slice offsets: every chain's N3 time slices, chain by chain (the
+        # smeared handle), and per blocked group in the blocked outputs
+        slice_at = np.concatenate([[0], np.cumsum([e[3] for e in extents])]).astype(int)
+        blocked_at, k = {}, 0
+        for gi in blocked_groups:
+            blocked_at[gi] = k
+            k += sum(extents[c][3] for c in per_group[gi])
         try:
             t0 = time.perf_counter()
             ens.metropolis_sweeps(proposal_angle, thermalization)
@@ -264,23 +272,24 @@ def scalar_glueball_pipeline(groups: Sequence[Tuple[int, Sequence[int]]] = ((128
                 ens.synchronize()
                 t1 = time.perf_counter()
                 res.sweep_seconds += t1 - t0
-                # levels are sequential, so each count continues from the
-                # previous one (0, 5, 10 costs 10 levels, not 15), bit for
-                # bit the same links as smearing from scratch
-                ens.copy_to(sm)
-                done = 0
-                for levels in sorted(stout_levels):
-                    if levels > done:
-                        sm.stout_smear_into(sm, rho, levels - done, lift_level_cap=True)
-                        done = levels
-                    basis = sm.scalar_operator_basis()
+                # one captured graph: the levels continue from the previous
+                # count (0, 5, 10 costs 10 levels, not 15; the same links as
+                # smearing from scratch), operators after each count, the
+                # blockable groups blocked and measured
+                levels_sorted = sorted(stout_levels)
+                plaq, rect, bplaq, brect = ens.glueball_measure(
+                    sm, levels_sorted, rho, [(subs[gi], coarse[gi], per_group[gi][0]) for gi in blocked_groups])
+                for li, levels in enumerate(levels_sorted):
                     for gi, chains in enumerate(per_group):
-                        samples.setdefault((gi, levels, False), []).extend(basis[c] for c in chains)
+                        samples.setdefault((gi, levels, False), []).extend(
+                            (plaq[li, slice_at[c]:slice_at[c] + extents[c][3]].copy(),
+                             rect[li, slice_at[c]:slice_at[c] + extents[c][3]].copy()) for c in chains)
                         if gi in subs:
-                            sm.copy_subset_to(chains, subs[gi])
-                            subs[gi].block_into(coarse[gi])
+                            k0 = blocked_at[gi]
                             samples.setdefault((gi, levels, True), []).extend(
-                                coarse[gi].scalar_operator_basis())
+                                (bplaq[li, k0 + j * extents[c][3]:k0 + (j + 1) * extents[c][3]].copy(),
+                                 brect[li, k0 + j * extents[c][3]:k0 + (j + 1) * extents[c][3]].copy())
+                                for j, c in enumerate(chains))
                 res.measure_seconds += time.perf_counter() - t1
         finally:
             for h in list(coarse.values()) + list(subs.values()) + [sm]:
