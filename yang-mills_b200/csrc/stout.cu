@@ -81,17 +81,11 @@ __device__ __forceinline__ bool from_algebra(const double coef[8], m3 &out) {
         if (squarings > 32) return false;
         scaled_norm *= 0.5;
     }
-    const double sc = ldexp(1.0, -squarings);
-    cplx h, d;
-    double nx, nx2;
-    {
-        const m3 x = scale_r(m, sc);
-        const m3 x2 = mul(x, x);
-        h = cmake(0.5 * trace3(x2).re, 0.5 * trace3(x2).im);
-        d = det3(x);
-        nx = max_abs(x);
-        nx2 = max_abs(x2);
-    }
+    const m3 x = scale_r(m, ldexp(1.0, -squarings));
+    const m3 x2 = mul(x, x);
+    const cplx h = cmake(0.5 * trace3(x2).re, 0.5 * trace3(x2).im);
+    const cplx d = det3(x);
+    const double nx = max_abs(x), nx2 = max_abs(x2);
     cplx an = cmake(1.0, 0.0), bn = cmake(0.0, 0.0), cn = cmake(0.0, 0.0);
     cplx f0 = an, f1 = bn, f2 = cn;
     for (int order = 1; order <= kMaxOrder; ++order) {
@@ -110,10 +104,6 @@ __device__ __forceinline__ bool from_algebra(const double coef[8], m3 &out) {
                              (fabs(tc.re) + fabs(tc.im)) * nx2;
         if (bound <= 1.0e-18) break;
     }
-    // x and x^2 are rebuilt here (the same operations, so the same values)
-    // rather than held in registers through the series
-    const m3 x = scale_r(m, sc);
-    const m3 x2 = mul(x, x);
     m3 sum;
 #pragma unroll
     for (int i = 0; i < 3; ++i)
@@ -173,7 +163,8 @@ k_stout_level(const ChainInfo *__restrict__ chains, const Tile *__restrict__ til
         const m3 staple = scale_r(sum, rho);
         if (!finite3(staple)) { atomicOr(err, kErrNonFiniteStaple); continue; }
         // stout_q (glueball_smearing.rs:174-193)
-        const m3 omega = mul_adj(staple, load_su3(in, c, s, mu));
+        const m3 old = load_su3(in, c, s, mu);
+        const m3 omega = mul_adj(staple, old);
         if (!finite3(omega)) { atomicOr(err, kErrNonFiniteStaple); continue; }
         const m3 anti = sub3(adj(omega), omega);
         const m3 firstq = scale_c(anti, cmake(0.0, 0.5));
@@ -212,7 +203,7 @@ k_stout_level(const ChainInfo *__restrict__ chains, const Tile *__restrict__ til
         if (!ok) { atomicOr(err, kErrProjection); continue; }
         m3 rot;
         if (!from_algebra(coef, rot) || !in_su3(rot)) { atomicOr(err, kErrGroup); continue; }
-        const m3 upd = mul(rot, load_su3(in, c, s, mu));   // reloaded (L1), not held
+        const m3 upd = mul(rot, old);
         if (!in_su3(upd)) { atomicOr(err, kErrGroup); continue; }
         store_su3(out, c, s, mu, upd);
     }
