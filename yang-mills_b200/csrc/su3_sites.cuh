@@ -47,13 +47,6 @@ __device__ __forceinline__ double block_reduce(double v) {
 // two matrix products as fma() chains (within 1e-12 relative of the
 // reference's plaquette; the tiled and chain-resident paths share this code
 // and so agree bitwise).
-// L1 prefetch of the nine entries of link (s, mu) (no registers held).
-__device__ __forceinline__ void prefetch_link_l1(const double2 *links, const ChainInfo &c, int64_t s, int mu) {
-    const double2 *p = links + c.offset + (int64_t)(mu * 9) * c.volume + s;
-#pragma unroll
-    for (int e = 0; e < 9; ++e) asm volatile("prefetch.global.L1 [%0];" ::"l"(p + (int64_t)e * c.volume));
-}
-
 template <bool RESIDENT>
 __device__ __forceinline__ double site_plaquette_sum(const double2 *links, const ChainInfo &c,
                                                      int64_t s) {
@@ -66,18 +59,6 @@ __device__ __forceinline__ double site_plaquette_sum(const double2 *links, const
         const Nb pm = step(c, x.x, x.lex, x.par, mu, +1);
 #pragma unroll 1
         for (int nu = mu + 1; nu < 4; ++nu) {
-#ifdef YM_PLAQ_PREFETCH
-            if (!RESIDENT) {
-                // the next plane's two neighbour links, while this plane runs
-                const int nmu = nu == 3 ? mu + 1 : mu, nnu = nu == 3 ? mu + 2 : nu + 1;
-                if (nmu < 3) {
-                    const Nb npm = step_any(c, x.x, x.lex, x.par, nmu, +1);
-                    const Nb npn = step_any(c, x.x, x.lex, x.par, nnu, +1);
-                    prefetch_link_l1(links, c, storage_index(c, npm.lex, npm.par), nnu);
-                    prefetch_link_l1(links, c, storage_index(c, npn.lex, npn.par), nmu);
-                }
-            }
-#endif
             const Nb pn = step(c, x.x, x.lex, x.par, nu, +1);
             m3 p = mul_fma(umu, link_at<RESIDENT>(links, c, storage_index(c, pm.lex, pm.par), nu));
             p = mul_adj_fma(p, link_at<RESIDENT>(links, c, storage_index(c, pn.lex, pn.par), mu));
