@@ -89,7 +89,7 @@ def measured_peaks():
 
 
 def ncu_traffic_per_launch():
-    """DRAM bytes per k_su3_metropolis launch from the committed ncu summary,
+    """DRAM bytes per k_su3_metropolis_ring launch from the committed ncu summary,
     scaled to a 32^4 launch (None when no summary exists)."""
     path = os.path.join(ROOT, "profiles", "su3_metropolis_32x4_fp64.md")
     try:
@@ -364,7 +364,7 @@ def main():
     ms, plaq = leg["ms"], leg["plaq"]
     roofline = dict(leg["roofline"])
     roofline.update({"traffic": ncu_traffic_per_launch(),
-                     "kernel": "k_su3_metropolis (one checkerboard sub-sweep)"})
+                     "kernel": "k_su3_metropolis_ring (ordered hits; one checkerboard sub-sweep)"})
 
     # spatial stout smearing of a 32^4 FP64 lattice (rho 0.1), each level
     # timed by its CUDA-event pair; compulsory traffic per level: every link

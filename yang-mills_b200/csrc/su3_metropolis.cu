@@ -544,9 +544,9 @@ __device__ __forceinline__ unsigned visit_ordered(m3 &u, const double2 (*sa)[T],
     return accepted;
 }
 
-// K: 0 = visit() (drawn generators); 13 / 16 = visit_ordered for half
-// widths <= 0.3 / <= 1.
-template <int MU, int K>
+// Drawn generators (visit()): three CTAs per SM, the accumulator in shared
+// memory, one staple term staged ahead.
+template <int MU>
 __global__ void __launch_bounds__(T, YM_METRO_MIN_BLOCKS)
 k_su3_metropolis(const ChainInfo *__restrict__ chains, const Tile *__restrict__ tiles,
                  double2 *__restrict__ links, int parity, double angle, int uniform,
@@ -575,8 +575,134 @@ k_su3_metropolis(const ChainInfo *__restrict__ chains, const Tile *__restrict__ 
         cp_async_wait_all();
         m3 u = staged_link(bufs.l1);
         const uint64_t key = link_key(c.seed, sweep, x.lex, MU);
-        accepted = K ? visit_ordered<K ? K : 13>(u, sa, c.beta / 3.0, angle, key)
-                     : visit(u, sa, c.beta / 3.0, angle, key, uniform);
+        accepted = visit(u, sa, c.beta / 3.0, angle, key, uniform);
+        store_su3(links, c, s, MU, u);
+    }
+    const unsigned warp_sum = __reduce_add_sync(0xffffffffu, accepted);
+    if ((threadIdx.x & 31) == 0 && warp_sum)
+        atomicAdd(accepts + tile.chain, (unsigned long long)warp_sum);
+}
+
+// ---- ordered hits: two staple terms in flight, two CTAs per SM -----------
+// The ordered-hit sub-sweep keeps the staple accumulator in registers and a
+// ring of two three-factor staging sets, so term k+2's factors are loading
+// while term k multiplies (one term ahead in k_su3_metropolis).  Two
+// 128-thread CTAs per SM fit (registers and 108 KB of staging each); after
+// the staple the accumulator is written once to the second set's memory for
+// the hits.  The products and their order are staple_pipelined's, so A has
+// the same bits.  On a 32^4 lattice this is 1.4 % faster than the
+// three-CTA form with the ordered visit, and 20 % slower with the drawn
+// generators' visit, whose loop-carried hits need the third CTA's warps.
+struct TermSet {
+    double2 (*f[3])[T];
+};
+
+template <int MU, int NU>
+__device__ __forceinline__ void stage_term3(const TermSet &b, const double2 *links, const ChainInfo &c,
+                                            const TermSites &t) {
+    const double2 *p1 = links + c.offset + (int64_t)(NU * 9) * c.volume + t.s1;
+    const double2 *p2 = links + c.offset + (int64_t)(MU * 9) * c.volume + t.s2;
+    const double2 *p3 = links + c.offset + (int64_t)(NU * 9) * c.volume + t.s3;
+#pragma unroll
+    for (int e = 0; e < 9; ++e) {
+        cp_async16(&b.f[0][e][threadIdx.x], p1 + (int64_t)e * c.volume);
+        cp_async16(&b.f[1][e][threadIdx.x], p2 + (int64_t)e * c.volume);
+        cp_async16(&b.f[2][e][threadIdx.x], p3 + (int64_t)e * c.volume);
+    }
+    cp_async_commit();
+}
+
+template <bool BWD>
+__device__ __forceinline__ void term_accumulate(const TermSet &b, m3 &a) {
+    m3 p;
+    {
+        const m3 l1 = staged_link(b.f[0]), l2 = staged_link(b.f[1]);
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                cplx v = cmake(0.0, 0.0);
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    if (!BWD) cfma(v, l1.e[r][j], cconj(l2.e[k][j]));
+                    else cfma(v, cconj(l1.e[j][r]), cconj(l2.e[k][j]));
+                }
+                p.e[r][k] = v;
+            }
+    }
+    const m3 l3 = staged_link(b.f[2]);
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int col = 0; col < 3; ++col)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                if (!BWD) cfma(a.e[r][col], p.e[r][k], cconj(l3.e[col][k]));
+                else cfma(a.e[r][col], p.e[r][k], l3.e[k][col]);
+            }
+}
+
+template <int MU>
+__device__ __forceinline__ m3 staple_ring(const double2 *links, const ChainInfo &c, const Coord &x, int par,
+                                          const Nb &pm, const TermSet &s0, const TermSet &s1, int64_t s_self) {
+    constexpr int N0 = Nu<MU, 0>::v, N1 = Nu<MU, 1>::v, N2 = Nu<MU, 2>::v;
+    stage_term3<MU, N0>(s0, links, c, term_sites<MU, N0, false>(c, x, par, pm));
+    stage_term3<MU, N0>(s1, links, c, term_sites<MU, N0, true>(c, x, par, pm));
+    m3 a;
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) a.e[r][k] = cmake(0.0, 0.0);
+    cp_async_wait_one();
+    term_accumulate<false>(s0, a);
+    stage_term3<MU, N1>(s0, links, c, term_sites<MU, N1, false>(c, x, par, pm));
+    cp_async_wait_one();
+    term_accumulate<true>(s1, a);
+    stage_term3<MU, N1>(s1, links, c, term_sites<MU, N1, true>(c, x, par, pm));
+    cp_async_wait_one();
+    term_accumulate<false>(s0, a);
+    stage_term3<MU, N2>(s0, links, c, term_sites<MU, N2, false>(c, x, par, pm));
+    cp_async_wait_one();
+    term_accumulate<true>(s1, a);
+    stage_term3<MU, N2>(s1, links, c, term_sites<MU, N2, true>(c, x, par, pm));
+    cp_async_wait_one();
+    term_accumulate<false>(s0, a);
+    stage_link(s0.f[0], links, c, s_self, MU);   // the updated link itself
+    cp_async_wait_one();
+    term_accumulate<true>(s1, a);
+    return a;
+}
+
+constexpr int kRingBuffers = 6;   // two sets of three factors
+
+template <int MU, int K>
+__global__ void __launch_bounds__(T, 2)
+k_su3_metropolis_ring(const ChainInfo *__restrict__ chains, const Tile *__restrict__ tiles,
+                      double2 *__restrict__ links, int parity, double angle,
+                      const uint64_t *__restrict__ sweep_ptr, unsigned long long *__restrict__ accepts,
+                      int log2_item) {
+    extern __shared__ __align__(16) double2 ring_mem[];
+    auto buf = [&](int i) { return reinterpret_cast<double2 (*)[T]>(ring_mem + (size_t)i * 9 * T); };
+    const TermSet s0{{buf(0), buf(1), buf(2)}}, s1{{buf(3), buf(4), buf(5)}};
+    const Tile tile = tiles[(int64_t)blockIdx.x * (T >> log2_item) + (threadIdx.x >> log2_item)];
+    const bool live = tile.chain >= 0;
+    const ChainInfo c = chains[live ? tile.chain : 0];
+    const int64_t t = tile.start + (threadIdx.x & ((1u << log2_item) - 1u));
+    const uint64_t sweep = *sweep_ptr;
+    unsigned accepted = 0;
+    if (live && t < c.half) {
+        const int64_t s = (int64_t)parity * c.half + t;
+        const Coord x = decode_storage(c, s);
+        const Nb pm = step(c, x.x, x.lex, parity, MU, +1);
+        const m3 a = staple_ring<MU>(links, c, x, parity, pm, s0, s1, s);
+        cp_async_wait_all();
+        m3 u = staged_link(s0.f[0]);
+        // the accumulator, for the hits, in the second set's (now free) memory
+        double2 (*sa)[T] = s1.f[0];
+#pragma unroll
+        for (int e = 0; e < 9; ++e) sa[e][threadIdx.x] = make_double2(a.e[e / 3][e % 3].re, a.e[e / 3][e % 3].im);
+        const uint64_t key = link_key(c.seed, sweep, x.lex, MU);
+        accepted = visit_ordered<K>(u, sa, c.beta / 3.0, angle, key);
         store_su3(links, c, s, MU, u);
     }
     const unsigned warp_sum = __reduce_add_sync(0xffffffffu, accepted);
@@ -903,19 +1029,41 @@ __global__ void k_advance_sweep(uint64_t *sweep) { *sweep += 1; }
 
 constexpr size_t kStageBytes = 27 * T * sizeof(double2);   // three staged factors per thread
 
+constexpr size_t kRingBytes = (size_t)kRingBuffers * 9 * T * sizeof(double2);
+
+// Both launchers take the handle's sweep layout: work items of 2^log2
+// sites, chain order or by descending chain volume (all layouts give the
+// same bits).
 template <int K>
-static void metro_launch(ym_ensemble *e, int parity, int mu, double angle, int uniform) {
-    // the handle's sweep layout: work items of 2^log2 sites, chain order or
-    // by descending chain volume (all layouts give the same bits)
+static void metro_launch_ordered(ym_ensemble *e, int parity, int mu, double angle) {
     const SweepLayout &L = e->layouts[e->sweep_layout];
     const dim3 grid((unsigned)L.ctas), block(T);
     const Tile *items = L.d_items;
     switch (mu) {
-    case 0: k_su3_metropolis<0, K><<<grid, block, kStageBytes, e->stream>>>(e->d_chains, items, e->d_links, parity, angle, uniform, e->d_sweep, e->d_accepts, L.log2_item); break;
-    case 1: k_su3_metropolis<1, K><<<grid, block, kStageBytes, e->stream>>>(e->d_chains, items, e->d_links, parity, angle, uniform, e->d_sweep, e->d_accepts, L.log2_item); break;
-    case 2: k_su3_metropolis<2, K><<<grid, block, kStageBytes, e->stream>>>(e->d_chains, items, e->d_links, parity, angle, uniform, e->d_sweep, e->d_accepts, L.log2_item); break;
-    default: k_su3_metropolis<3, K><<<grid, block, kStageBytes, e->stream>>>(e->d_chains, items, e->d_links, parity, angle, uniform, e->d_sweep, e->d_accepts, L.log2_item); break;
+    case 0: k_su3_metropolis_ring<0, K><<<grid, block, kRingBytes, e->stream>>>(e->d_chains, items, e->d_links, parity, angle, e->d_sweep, e->d_accepts, L.log2_item); break;
+    case 1: k_su3_metropolis_ring<1, K><<<grid, block, kRingBytes, e->stream>>>(e->d_chains, items, e->d_links, parity, angle, e->d_sweep, e->d_accepts, L.log2_item); break;
+    case 2: k_su3_metropolis_ring<2, K><<<grid, block, kRingBytes, e->stream>>>(e->d_chains, items, e->d_links, parity, angle, e->d_sweep, e->d_accepts, L.log2_item); break;
+    default: k_su3_metropolis_ring<3, K><<<grid, block, kRingBytes, e->stream>>>(e->d_chains, items, e->d_links, parity, angle, e->d_sweep, e->d_accepts, L.log2_item); break;
     }
+}
+
+static void metro_launch_drawn(ym_ensemble *e, int parity, int mu, double angle) {
+    const SweepLayout &L = e->layouts[e->sweep_layout];
+    const dim3 grid((unsigned)L.ctas), block(T);
+    const Tile *items = L.d_items;
+    switch (mu) {
+    case 0: k_su3_metropolis<0><<<grid, block, kStageBytes, e->stream>>>(e->d_chains, items, e->d_links, parity, angle, 1, e->d_sweep, e->d_accepts, L.log2_item); break;
+    case 1: k_su3_metropolis<1><<<grid, block, kStageBytes, e->stream>>>(e->d_chains, items, e->d_links, parity, angle, 1, e->d_sweep, e->d_accepts, L.log2_item); break;
+    case 2: k_su3_metropolis<2><<<grid, block, kStageBytes, e->stream>>>(e->d_chains, items, e->d_links, parity, angle, 1, e->d_sweep, e->d_accepts, L.log2_item); break;
+    default: k_su3_metropolis<3><<<grid, block, kStageBytes, e->stream>>>(e->d_chains, items, e->d_links, parity, angle, 1, e->d_sweep, e->d_accepts, L.log2_item); break;
+    }
+}
+
+static cudaError_t set_smem(const void *f, size_t bytes) {
+    cudaError_t err = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (err == cudaSuccess)
+        err = cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+    return err;
 }
 
 cudaError_t launch_su3_metropolis(ym_ensemble *e, int parity, int mu, double angle, int uniform) {
@@ -923,26 +1071,23 @@ cudaError_t launch_su3_metropolis(ym_ensemble *e, int parity, int mu, double ang
     int dev = 0;
     cudaGetDevice(&dev);
     if (configured_device != dev) {
-        const void *fns[12] = {(const void *)k_su3_metropolis<0, 0>, (const void *)k_su3_metropolis<1, 0>,
-                               (const void *)k_su3_metropolis<2, 0>, (const void *)k_su3_metropolis<3, 0>,
-                               (const void *)k_su3_metropolis<0, 13>, (const void *)k_su3_metropolis<1, 13>,
-                               (const void *)k_su3_metropolis<2, 13>, (const void *)k_su3_metropolis<3, 13>,
-                               (const void *)k_su3_metropolis<0, 16>, (const void *)k_su3_metropolis<1, 16>,
-                               (const void *)k_su3_metropolis<2, 16>, (const void *)k_su3_metropolis<3, 16>};
-        for (const void *f : fns) {
-            cudaError_t err = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageBytes);
-            if (err == cudaSuccess)
-                err = cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                           cudaSharedmemCarveoutMaxShared);
-            if (err != cudaSuccess) return err;
-        }
+        const void *drawn[4] = {(const void *)k_su3_metropolis<0>, (const void *)k_su3_metropolis<1>,
+                                (const void *)k_su3_metropolis<2>, (const void *)k_su3_metropolis<3>};
+        const void *ordered[8] = {(const void *)k_su3_metropolis_ring<0, 13>, (const void *)k_su3_metropolis_ring<1, 13>,
+                                  (const void *)k_su3_metropolis_ring<2, 13>, (const void *)k_su3_metropolis_ring<3, 13>,
+                                  (const void *)k_su3_metropolis_ring<0, 16>, (const void *)k_su3_metropolis_ring<1, 16>,
+                                  (const void *)k_su3_metropolis_ring<2, 16>, (const void *)k_su3_metropolis_ring<3, 16>};
+        for (const void *f : drawn)
+            if (cudaError_t err = set_smem(f, kStageBytes)) return err;
+        for (const void *f : ordered)
+            if (cudaError_t err = set_smem(f, kRingBytes)) return err;
         configured_device = dev;
     }
     // ordered hits: the pipelined visit with the term count the half width
     // allows (angles are validated to lie in [1e-8, 1] for binary64 handles)
-    if (uniform) metro_launch<0>(e, parity, mu, angle, uniform);
-    else if (angle <= 0.3) metro_launch<13>(e, parity, mu, angle, uniform);
-    else metro_launch<16>(e, parity, mu, angle, uniform);
+    if (uniform) metro_launch_drawn(e, parity, mu, angle);
+    else if (angle <= 0.3) metro_launch_ordered<13>(e, parity, mu, angle);
+    else metro_launch_ordered<16>(e, parity, mu, angle);
     return cudaGetLastError();
 }
 
