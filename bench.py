@@ -10,7 +10,9 @@ average-plaquette measurement.  The lattice (604 MB) is larger than the
 126 MB L2, so no flush is needed between steps.  ``value`` is link updates/s
 (one link visit = eight proposals) over all GPUs.
 
-Beside it: the same steps with two-row binary32 links (``fp32_two_row``),
+Beside it: the same FP64 steps in the fast form (``fp64_fast``: fused
+multiply-adds and Horner rotations, with its distance from the exact form
+after ten sweeps), the same steps with two-row binary32 links (``fp32_two_row``),
 with the learned proposal (``learned``: its network trained on the GPU on
 2000 configurations of the plain sampler), and the plaquette ESS/s of plain
 FP64, plain FP32 (half width 0.3 and, as a control, the widest the
@@ -52,6 +54,7 @@ TRAIN_STEPS = 2000                    # configurations the plain sampler generat
 TRAIN_LR = 3e-3
 LOOP_BLOCKS = 10                      # loop measurements per run of the loop cadence
 LOOP_EVERY = 10                       # sweeps between Wilson / Polyakov measurements
+FAST_CHECK_SWEEPS = 10                # sweeps per form when the fast form is compared with the exact one
 MASTER_SEED = 0x2C02198105010002
 LINK_BYTES = 144                      # FP64 3x3 complex
 LINKS_PER_UPDATE = 9                  # 8 link reads + 1 write per checkerboard update
@@ -366,6 +369,33 @@ def main():
     roofline.update({"traffic": ncu_traffic_per_launch(),
                      "kernel": "k_su3_metropolis_ring (ordered hits; one checkerboard sub-sweep)"})
 
+    # the same FP64 step in the fast form (fused multiply-adds, Horner
+    # rotations; ym_ensemble_set_fast_sweeps) from a copy of the same lattice,
+    # then its distance from the exact form: two copies of the lattice after
+    # that leg, ten sweeps each from the same sweep index, exact and fast
+    fast_src = ens.like()
+    ens.copy_to(fast_src)
+    fast_src.sweep_index = ens.sweep_index
+    fast_src.fast_sweeps = True
+    fleg = timed_leg(fast_src, lambda: fast_src.metropolis_sweeps(ANGLE, 1), LINK_BYTES, "su3_metropolis")
+    pair = []
+    for fast in (False, True):
+        c = fast_src.like()
+        fast_src.copy_to(c)
+        c.sweep_index = fast_src.sweep_index
+        c.fast_sweeps = fast
+        c.reset_accounting()
+        c.metropolis_sweeps(ANGLE, FAST_CHECK_SWEEPS, "ordered")
+        pair.append((c.download(0), int(c.accounting()[1][0]), float(c.average_plaquette()[0])))
+        c.close()
+    fast_src.close()
+    fast_err = {
+        "sweeps": FAST_CHECK_SWEEPS, "lattice": "32^4, the bench lattice after the fast leg",
+        "max_abs_link_entry_difference": float(np.max(np.abs(pair[0][0] - pair[1][0]))),
+        "accepts_exact": pair[0][1], "accepts_fast": pair[1][1],
+        "plaquette_difference": pair[1][2] - pair[0][2]}
+    del pair
+
     # spatial stout smearing of a 32^4 FP64 lattice (rho 0.1), each level
     # timed by its CUDA-event pair; compulsory traffic per level: every link
     # of every site read once and written once.  The reference's smearing
@@ -679,6 +709,14 @@ def main():
                 "step": "1 checkerboard sweep + FP64 reunitarisation + average plaquette",
                 "plaquette_mean": float(np.mean(f32["plaq"])), "acceptance": f32["acceptance"],
                 "roofline": f32["roofline"]},
+            "fp64_fast": {
+                "value": fleg["value"], "unit": UNIT, "ms_per_step": fleg["ms"] / args.steps,
+                "dtype": "f64 (fused multiply-adds, Horner rotations)",
+                "step": "1 checkerboard sweep (fast form) + average plaquette",
+                "plaquette_mean": float(np.mean(fleg["plaq"])), "acceptance": fleg["acceptance"],
+                "roofline": dict(fleg["roofline"], kernel="tiled_fast::k_su3_metropolis_ring "
+                                                          "(ordered hits; one sub-sweep)"),
+                "error_vs_exact": fast_err},
             "learned": {
                 "value": lrn["value"], "unit": UNIT, "ms_per_step": lrn["ms"] / args.steps,
                 "dtype": "f32 links, bf16 network (fp32 accumulate), f64 dS/accept/plaquette",

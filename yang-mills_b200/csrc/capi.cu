@@ -244,7 +244,7 @@ cudaError_t time_on_stream(ym_ensemble *e, F run, float *ms) {
 // each sub-sweep keeps its event pair.
 bool resident_candidate(const ym_ensemble *e) {
     return e->group == YM_GROUP_SU3 && e->precision == YM_PREC_F64 && !e->profiling &&
-           e->resident_choice != 0 && ym::resident_fits(e);
+           !e->fast_sweeps && e->resident_choice != 0 && ym::resident_fits(e);
 }
 
 constexpr int64_t kTuneSweeps = 4;   // sweeps timed per path when choosing
@@ -253,17 +253,22 @@ constexpr int64_t kTuneSweeps = 4;   // sweeps timed per path when choosing
 // launched without graph replay) are then at most half of the call.
 constexpr int64_t kLayoutTuneMin = 2 * (ym::kSweepLayouts * kTuneSweeps + 1);
 
-// Selects sub-sweep layout li; captured graphs hold the previous layout's
-// launches, so they are dropped when it changes.
-void set_layout(ym_ensemble *e, int32_t li) {
-    if (e->sweep_layout == li && e->layout_tuned) return;
-    e->sweep_layout = li;
+// Captured sweep graphs hold the launches of one layout and one form of the
+// sub-sweep kernels; they are dropped when either changes.
+void drop_sweep_graphs(ym_ensemble *e) {
     if (e->sweep_graph) cudaGraphExecDestroy(e->sweep_graph);
     e->sweep_graph = nullptr;
     if (e->measure_graph) cudaGraphExecDestroy(e->measure_graph);
     e->measure_graph = nullptr;
     if (e->run_graph) cudaGraphExecDestroy(e->run_graph);
     e->run_graph = nullptr;
+}
+
+// Selects sub-sweep layout li.
+void set_layout(ym_ensemble *e, int32_t li) {
+    if (e->sweep_layout == li && e->layout_tuned) return;
+    e->sweep_layout = li;
+    drop_sweep_graphs(e);
 }
 
 }  // namespace
@@ -920,13 +925,29 @@ int32_t ym_ensemble_lift_angle_cap(ym_ensemble *e, int32_t lift) {
     return YM_OK;
 }
 
+int32_t ym_ensemble_set_fast_sweeps(ym_ensemble *e, int32_t on) {
+    if (!e) return YM_ERR_NULL_ARGUMENT;
+    if (on != 0 && on != 1) return YM_ERR_INVALID_ARGUMENT;
+    if (on && (e->group != YM_GROUP_SU3 || e->precision != YM_PREC_F64)) return YM_ERR_UNSUPPORTED_PRECISION;
+    if (e->fast_sweeps == (on != 0)) return YM_OK;
+    e->fast_sweeps = on != 0;
+    drop_sweep_graphs(e);
+    return YM_OK;
+}
+
+int32_t ym_ensemble_get_fast_sweeps(ym_ensemble *e, int32_t *on) {
+    if (!e || !on) return YM_ERR_NULL_ARGUMENT;
+    *on = e->fast_sweeps ? 1 : 0;
+    return YM_OK;
+}
+
 int32_t ym_ensemble_set_sweep_path(ym_ensemble *e, int32_t path) {
     if (!e) return YM_ERR_NULL_ARGUMENT;
     if (path != YM_PATH_AUTO && path != YM_PATH_TILED && path != YM_PATH_RESIDENT) return YM_ERR_INVALID_ARGUMENT;
     if (path == YM_PATH_RESIDENT) {
         int32_t st = set_device(e);
         if (st) return st;
-        if (e->group != YM_GROUP_SU3 || e->precision != YM_PREC_F64 || !ym::resident_fits(e))
+        if (e->group != YM_GROUP_SU3 || e->precision != YM_PREC_F64 || e->fast_sweeps || !ym::resident_fits(e))
             return YM_ERR_INVALID_ARGUMENT;
     }
     e->resident_choice = path;

@@ -112,6 +112,9 @@ struct ym_ensemble {
     bool layout_tuned = false;
     // Half widths above the reference's 1.0 admitted (two-row handles only).
     bool angle_cap_lifted = false;
+    // SU(3) FP64 sweeps in the fast form (fused multiply-adds, Horner
+    // rotations; su3_metropolis_fast.cu) instead of the reference's bits.
+    bool fast_sweeps = false;
     // Captured block of the loop-measurement cadence (ym_su3_measured_run):
     // sweeps with a plaquette each, then Wilson and Polyakov loops.
     cudaGraphExec_t run_graph = nullptr;
@@ -187,6 +190,9 @@ cudaError_t launch_su3_identity(ym_ensemble *e);
 cudaError_t launch_su3_from_aos(ym_ensemble *e, int64_t chain);
 cudaError_t launch_su3_to_aos(ym_ensemble *e, int64_t chain);
 cudaError_t launch_su3_metropolis(ym_ensemble *e, int parity, int mu, double angle, int uniform);
+// The same sub-sweep in the fast form (su3_metropolis_fast.cu);
+// launch_su3_metropolis dispatches to it when e->fast_sweeps is set.
+cudaError_t launch_su3_metropolis_fast(ym_ensemble *e, int parity, int mu, double angle, int uniform);
 cudaError_t launch_advance_sweep(ym_ensemble *e);
 // Chain-resident sweeps (su3_metropolis.cu): every chain small enough that
 // its links fit in one CTA's shared memory.  series (device, may be null)

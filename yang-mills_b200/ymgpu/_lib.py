@@ -51,6 +51,8 @@ SIGNATURES = {
     "ym_su3_accounting": [VP, P(u64), P(u64)],
     "ym_ensemble_set_sweep_path": [VP, i32],
     "ym_ensemble_lift_angle_cap": [VP, i32],
+    "ym_ensemble_set_fast_sweeps": [VP, i32],
+    "ym_ensemble_get_fast_sweeps": [VP, P(i32)],
     "ym_ensemble_set_sweep_layout": [VP, i32, i32],
     "ym_ensemble_get_sweep_layout": [VP, P(i32), P(i32), P(i32)],
     "ym_ensemble_get_sweep_path": [VP, P(i32)],

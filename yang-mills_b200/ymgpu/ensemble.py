@@ -194,6 +194,19 @@ class Ensemble:
         check(lib().ym_ensemble_lift_angle_cap(self._h, int(lift)), "lift_angle_cap")
 
     @property
+    def fast_sweeps(self) -> bool:
+        """Whether SU(3) FP64 sweeps run in the fast form (fused
+        multiply-adds, Horner rotations; a few ulps per update from the
+        reference's bits, include/ymgpu.h) instead of the exact one."""
+        v = C.c_int32()
+        check(lib().ym_ensemble_get_fast_sweeps(self._h, C.byref(v)), "get_fast_sweeps")
+        return bool(v.value)
+
+    @fast_sweeps.setter
+    def fast_sweeps(self, on: bool) -> None:
+        check(lib().ym_ensemble_set_fast_sweeps(self._h, int(bool(on))), "set_fast_sweeps")
+
+    @property
     def sweep_path(self) -> str:
         """'auto' (undecided), 'tiled' or 'resident' (include/ymgpu.h)."""
         v = C.c_int32()
