@@ -613,12 +613,15 @@ def main():
         secs = time.perf_counter() - t
         out["glueball_pipeline_128x4^3x10+64x6^3x12+32x8^3x16"] = {
             "seconds": secs, "sweep_seconds": r.sweep_seconds, "measure_seconds": r.measure_seconds,
+            "prepare_seconds": r.prepare_seconds,
             "link_updates_per_s_in_sweeps": r.link_updates / r.sweep_seconds,
             "surfaces": len(r.surfaces), "sweep_layout": r.sweep_layout, "sweep_path": r.sweep_path,
             "note": "64 thermalisation sweeps (the first 50 probe the sub-sweep layouts), "
                     "4 measurements 4 sweeps apart; each measurement stout 0/5/10 levels (rho 0.1, "
                     "smeared incrementally: 10 levels in all), stride-2 blocking of the 6^3 and 8^3 "
-                    "groups, A1++ operators; correlators, jackknife and covariance on the host"}
+                    "groups, A1++ operators; correlators, jackknife and covariance on the host; "
+                    "prepare_seconds: the measurement graph built and uploaded once before the "
+                    "first measurement"}
         # the reference's phase-3F production campaign (16 x 4^3x10, beta 5.7) with
         # its correlated fits, and the published-baseline acceptance harnesses
         from ymgpu import benchmarks as B

@@ -413,6 +413,12 @@ typedef struct {
 int32_t ym_su3_glueball_measure(ym_ensemble *ens, ym_ensemble *smeared, const ym_glueball_plan *plan,
                                 double *plaquette, double *rectangle, double *blocked_plaquette,
                                 double *blocked_rectangle);
+/* The set-up half of ym_su3_glueball_measure (no reference counterpart):
+ * validates the plan, allocates the handles' scratch, captures the
+ * measurement graph and uploads it, without measuring; a later
+ * ym_su3_glueball_measure with the same plan and handles only launches it.
+ * Production drivers call it once before their first measurement. */
+int32_t ym_su3_glueball_prepare(ym_ensemble *ens, ym_ensemble *smeared, const ym_glueball_plan *plan);
 
 /* ---- two-row binary32 storage (YM_PREC_F32_TWO_ROW, no reference
  * counterpart: the reference stores 18 doubles per link) ----

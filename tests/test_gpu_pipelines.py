@@ -180,3 +180,31 @@ def test_glueball_measurement_graph_equals_separate_calls(oracle):
         finally:
             for h in (fine, coarse, ref_sm, ref_fine, ref_coarse):
                 h.close()
+
+
+def test_glueball_prepare_then_measure_equals_measure():
+    """ym_su3_glueball_prepare builds and uploads the measurement graph
+    without measuring; the measurements after it equal those of a handle that
+    was never prepared, bit for bit, and preparing leaves the links alone."""
+    import ymgpu
+    from ymgpu import glueball as G
+    exts = [[4, 4, 4, 6]] * 2 + [[6, 6, 6, 4]] * 2
+    with ymgpu.Ensemble(exts, 5.7, [5, 6, 7, 8]) as ens:
+        ens.hot_start()
+        ens.metropolis_sweeps(1.0, 4, "uniform")
+        sms = [ens.like(), ens.like()]
+        fines = [sm.subset([2, 3]) for sm in sms]
+        coarses = [f.like([G.blocked_extents(e) for e in f.extents]) for f in fines]
+        try:
+            before = ens.download(0)
+            ens.glueball_prepare(sms[0], [0, 1, 3], 0.1, [(fines[0], coarses[0], 2)])
+            assert np.array_equal(before, ens.download(0))
+            for _ in range(2):
+                a = ens.glueball_measure(sms[0], [0, 1, 3], 0.1, [(fines[0], coarses[0], 2)])
+                b = ens.glueball_measure(sms[1], [0, 1, 3], 0.1, [(fines[1], coarses[1], 2)])
+                for x, y in zip(a, b):
+                    assert np.array_equal(x, y)
+                ens.metropolis_sweeps(0.35, 1, "ordered")
+        finally:
+            for h in fines + coarses + sms:
+                h.close()

@@ -1269,13 +1269,17 @@ int32_t ym_su3_spatial_stride2_block(ym_ensemble *src, ym_ensemble *dst) {
     return take_device_error(dst);
 }
 
-int32_t ym_su3_glueball_measure(ym_ensemble *ens, ym_ensemble *sm, const ym_glueball_plan *plan,
-                                double *plaquette, double *rectangle, double *blocked_plaquette,
-                                double *blocked_rectangle) {
-    if (!ens || !sm || !plan || !plaquette || !rectangle) return YM_ERR_NULL_ARGUMENT;
+}  // extern "C"
+
+// Validation, scratch and the captured measurement graph of `plan` (built on
+// the first call with these handles and levels, kept on `sm`); on return
+// sm->glueball_graph is ready to launch and need / blocked_slices give the
+// output layout.
+static int32_t glueball_graph(ym_ensemble *ens, ym_ensemble *sm, const ym_glueball_plan *plan, int64_t *need_out,
+                              int64_t *blocked_out) {
+    if (!ens || !sm || !plan) return YM_ERR_NULL_ARGUMENT;
     if (plan->n_levels < 1 || !plan->levels || plan->n_blocked < 0) return YM_ERR_INVALID_ARGUMENT;
-    if (plan->n_blocked > 0 && (!plan->fine || !plan->coarse || !plan->first_chain ||
-                                !blocked_plaquette || !blocked_rectangle))
+    if (plan->n_blocked > 0 && (!plan->fine || !plan->coarse || !plan->first_chain))
         return YM_ERR_NULL_ARGUMENT;
     { const int32_t g__ = require_su3_f64(ens); if (g__) return g__; }
     if (!same_geometry(ens, sm)) return YM_ERR_LATTICE_EXTENTS_MISMATCH;
@@ -1430,6 +1434,31 @@ int32_t ym_su3_glueball_measure(ym_ensemble *ens, ym_ensemble *sm, const ym_glue
         sm->glueball_key = key;
         sm->glueball_rho = plan->rho;
     }
+    *need_out = need;
+    *blocked_out = blocked_slices;
+    return YM_OK;
+}
+
+extern "C" {
+
+int32_t ym_su3_glueball_prepare(ym_ensemble *ens, ym_ensemble *sm, const ym_glueball_plan *plan) {
+    int64_t need = 0, blocked_slices = 0;
+    const int32_t st = glueball_graph(ens, sm, plan, &need, &blocked_slices);
+    if (st) return st;
+    YM_CUDA(cudaGraphUpload(sm->glueball_graph, sm->stream));
+    YM_CUDA(cudaStreamSynchronize(sm->stream));
+    return YM_OK;
+}
+
+int32_t ym_su3_glueball_measure(ym_ensemble *ens, ym_ensemble *sm, const ym_glueball_plan *plan,
+                                double *plaquette, double *rectangle, double *blocked_plaquette,
+                                double *blocked_rectangle) {
+    if (!ens || !sm || !plan || !plaquette || !rectangle) return YM_ERR_NULL_ARGUMENT;
+    if (plan->n_blocked > 0 && (!blocked_plaquette || !blocked_rectangle)) return YM_ERR_NULL_ARGUMENT;
+    int64_t need = 0, blocked_slices = 0;
+    int32_t st = glueball_graph(ens, sm, plan, &need, &blocked_slices);
+    if (st) return st;
+    const int64_t per_level = 2 * (sm->n_slices + blocked_slices);
     YM_CUDA(cudaGraphLaunch(sm->glueball_graph, sm->stream));
     std::vector<double> host((size_t)need);
     YM_CUDA(cudaMemcpyAsync(host.data(), sm->d_gb_series, (size_t)need * sizeof(double), cudaMemcpyDeviceToHost,

@@ -273,37 +273,49 @@ k_polyakov(const ChainInfo *__restrict__ chains, const Tile *__restrict__ tiles,
     }
 }
 
-// R x 1 rectangle (R along MU, one step along NU) from w0 as Re (1/3) Tr(P Q^dag)
-// with P = U_mu(x)..U_mu(x+(R-1)mu) U_nu(x+R mu) and Q = U_nu(x) U_mu(x+nu)..
-// U_mu(x+nu+(R-1)mu), the two halves of the closed path in traversal order
-// (fma chains): 2R products instead of the single chain's 2R + 1, each at
-// about half the FP64 instructions.
-template <int MU, int NU, int R>
-__device__ __forceinline__ double rect_pq(const double2 *links, const ChainInfo &c, const Walker &w0) {
-    Walker w = w0;
-    m3 pp = link_of(links, c, w, MU);
-#pragma unroll
-    for (int i = 1; i < R; ++i) {
-        step_walker(c, w, MU);
-        pp = mul_fma(pp, link_of(links, c, w, MU));
+// The 1x1 loop of spatial plane (A, B) and the 2x1 loops (A, B) and (B, A)
+// of one site, each as Re (1/3) Tr(P Q^dag) of the two halves of its closed
+// path in traversal order (fma chains): for an R x 1 rectangle (R along M,
+// one step along N) P = U_M(x)..U_M(x+(R-1)M) U_N(x+R M) and
+// Q = U_N(x) U_M(x+N)..U_M(x+N+(R-1)M), 2R products instead of the single
+// chain's 2R + 1.  The halves of the 1x1 loop are the corners
+// K_AB = U_A(x) U_B(x+A) and K_BA, and they are the first products of the
+// 2x1 loops' Q halves (Q of (A, B) is K_BA U_A(x+B+A), Q of (B, A) is
+// K_AB U_B(x+A+B)), so the three loops take 8 products instead of 10 with
+// every product the same.
+template <int A, int B>
+__device__ __forceinline__ void plane_loops(const double2 *links, const ChainInfo &c, const Walker &w0,
+                                            double &plaq, double &rect_ab, double &rect_ba) {
+    Walker wa = w0, wb = w0;
+    step_walker(c, wa, A);
+    step_walker(c, wb, B);
+    Walker wab = wa;
+    step_walker(c, wab, B);
+    const m3 kab = mul_fma(link_of(links, c, w0, A), link_of(links, c, wa, B));
+    const m3 kba = mul_fma(link_of(links, c, w0, B), link_of(links, c, wb, A));
+    plaq = retrace_mul_adj(kab, kba) * (1.0 / 3.0);
+    {
+        const m3 qq = mul_fma(kba, link_of(links, c, wab, A));
+        Walker w = wa;
+        step_walker(c, w, A);
+        const m3 pp = mul_fma(mul_fma(link_of(links, c, w0, A), link_of(links, c, wa, A)), link_of(links, c, w, B));
+        rect_ab = retrace_mul_adj(pp, qq) * (1.0 / 3.0);
     }
-    step_walker(c, w, MU);
-    pp = mul_fma(pp, link_of(links, c, w, NU));
-    w = w0;
-    m3 qq = link_of(links, c, w, NU);
-    step_walker(c, w, NU);
-#pragma unroll
-    for (int i = 0; i < R; ++i) {
-        qq = mul_fma(qq, link_of(links, c, w, MU));
-        step_walker(c, w, MU);
+    {
+        const m3 qq = mul_fma(kab, link_of(links, c, wab, B));
+        Walker w = wb;
+        step_walker(c, w, B);
+        const m3 pp = mul_fma(mul_fma(link_of(links, c, w0, B), link_of(links, c, wb, B)), link_of(links, c, w, A));
+        rect_ba = retrace_mul_adj(pp, qq) * (1.0 / 3.0);
     }
-    return retrace_mul_adj(pp, qq) * (1.0 / 3.0);
 }
 
 // Scalar operator basis, per site with x3 = t: sum of Re W over the three
 // 1x1 spatial orientations (0,1),(0,2),(1,2) and the six 2x1 orientations
 // (0,1),(0,2),(1,0),(1,2),(2,0),(2,1) (glueball_operators.rs:24-26), summed
 // in that order.
+// (250 registers, two blocks per SM: 0.52 ms at 32^4; capped at three
+// blocks, 168 registers with spills, 0.66 ms)
 __global__ void __launch_bounds__(T)
 k_operator_sites(const ChainInfo *__restrict__ chains, const Tile *__restrict__ tiles,
                  const double2 *__restrict__ links, double2 *__restrict__ site_vals) {
@@ -312,11 +324,12 @@ k_operator_sites(const ChainInfo *__restrict__ chains, const Tile *__restrict__ 
     const int64_t s = tile.start + threadIdx.x;
     if (s >= c.volume) return;
     const Walker w0 = walker_of(decode_storage(c, s));
-    const double p = (rect_pq<0, 1, 1>(links, c, w0) + rect_pq<0, 2, 1>(links, c, w0)) +
-                     rect_pq<1, 2, 1>(links, c, w0);
-    const double r = ((((rect_pq<0, 1, 2>(links, c, w0) + rect_pq<0, 2, 2>(links, c, w0)) +
-                        rect_pq<1, 0, 2>(links, c, w0)) + rect_pq<1, 2, 2>(links, c, w0)) +
-                      rect_pq<2, 0, 2>(links, c, w0)) + rect_pq<2, 1, 2>(links, c, w0);
+    double p01, p02, p12, r01, r10, r02, r20, r12, r21;
+    plane_loops<0, 1>(links, c, w0, p01, r01, r10);
+    plane_loops<0, 2>(links, c, w0, p02, r02, r20);
+    plane_loops<1, 2>(links, c, w0, p12, r12, r21);
+    const double p = (p01 + p02) + p12;
+    const double r = ((((r01 + r02) + r10) + r12) + r20) + r21;
     // indexed by the chain's storage slot
     site_vals[c.offset / 36 + s] = make_double2(p, r);
 }

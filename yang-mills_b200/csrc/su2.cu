@@ -396,12 +396,14 @@ k_su2_unit_residual(const ChainInfo *__restrict__ chains, const Tile *__restrict
     }
 }
 
-__global__ void k_su2_identity(double2 *links, int64_t offset, int64_t volume) {
-    const int64_t n = 8 * volume;
+// Every chain at once: blockIdx.y picks the chain.
+__global__ void k_su2_identity(const ChainInfo *__restrict__ chains, double2 *links) {
+    const ChainInfo c = chains[blockIdx.y];
+    const int64_t n = 8 * c.volume;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t plane = i / volume;
-        links[offset + i] = make_double2((plane % 2 == 0) ? 1.0 : 0.0, 0.0);
+        const int64_t plane = i / c.volume;
+        links[c.offset + i] = make_double2((plane % 2 == 0) ? 1.0 : 0.0, 0.0);
     }
 }
 
@@ -521,9 +523,13 @@ cudaError_t launch_su2_unit_residual_partials(ym_ensemble *e) {
 }
 
 cudaError_t launch_su2_identity(ym_ensemble *e) {
-    for (int64_t ch = 0; ch < e->n_chains; ++ch) {
-        const ChainInfo &c = e->chains[ch];
-        k_su2_identity<<<grid_for(8 * c.volume, 256), 256, 0, e->stream>>>(e->d_links, c.offset, c.volume);
+    int64_t vmax = 0;
+    for (const ChainInfo &c : e->chains) vmax = c.volume > vmax ? c.volume : vmax;
+    for (int64_t first = 0; first < e->n_chains; first += 65535) {   // the grid's y limit
+        const int64_t count = e->n_chains - first < 65535 ? e->n_chains - first : 65535;
+        const int64_t bx = (grid_for(8 * vmax, 256) + count - 1) / count;
+        k_su2_identity<<<dim3((unsigned)(bx < 1 ? 1 : bx), (unsigned)count), 256, 0, e->stream>>>(
+            e->d_chains + first, e->d_links);
     }
     return cudaGetLastError();
 }

@@ -128,12 +128,14 @@ k_f32_plaquette(const ChainInfo *__restrict__ chains, const Tile *__restrict__ t
     }
 }
 
-__global__ void k_f32_identity(float2 *links, int64_t offset, int64_t volume) {
-    const int64_t n = 24 * volume;
+// Every chain at once: blockIdx.y picks the chain.
+__global__ void k_f32_identity(const ChainInfo *__restrict__ chains, float2 *links) {
+    const ChainInfo c = chains[blockIdx.y];
+    const int64_t n = 24 * c.volume;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
-        const int e = (int)((i / volume) % 6);
-        links[offset + i] = make_float2((e == 0 || e == 4) ? 1.f : 0.f, 0.f);
+        const int e = (int)((i / c.volume) % 6);
+        links[c.offset + i] = make_float2((e == 0 || e == 4) ? 1.f : 0.f, 0.f);
     }
 }
 
@@ -255,9 +257,13 @@ cudaError_t launch_f32_plaquette_partials(ym_ensemble *e) {
 }
 
 cudaError_t launch_f32_identity(ym_ensemble *e) {
-    for (int64_t ch = 0; ch < e->n_chains; ++ch) {
-        const ChainInfo &c = e->chains[ch];
-        k_f32_identity<<<grid_for(24 * c.volume, 256), 256, 0, e->stream>>>(f32_links(e), c.offset, c.volume);
+    int64_t vmax = 0;
+    for (const ChainInfo &c : e->chains) vmax = c.volume > vmax ? c.volume : vmax;
+    for (int64_t first = 0; first < e->n_chains; first += 65535) {   // the grid's y limit
+        const int64_t count = e->n_chains - first < 65535 ? e->n_chains - first : 65535;
+        const int64_t bx = (grid_for(24 * vmax, 256) + count - 1) / count;
+        k_f32_identity<<<dim3((unsigned)(bx < 1 ? 1 : bx), (unsigned)count), 256, 0, e->stream>>>(
+            e->d_chains + first, f32_links(e));
     }
     return cudaGetLastError();
 }

@@ -229,12 +229,15 @@ cudaError_t launch_su3_hot_start(ym_ensemble *e) {
 
 // ------------------------------------------------------------ layout
 
-__global__ void k_su3_identity(double2 *links, int64_t offset, int64_t volume) {
-    const int64_t n = 36 * volume;
+// Every chain at once: blockIdx.y picks the chain, the blocks along x
+// stride over its 36 V entries.
+__global__ void k_su3_identity(const ChainInfo *__restrict__ chains, double2 *links) {
+    const ChainInfo c = chains[blockIdx.y];
+    const int64_t n = 36 * c.volume;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
-        const int entry = (int)((i / volume) % 9);
-        links[offset + i] = make_double2((entry == 0 || entry == 4 || entry == 8) ? 1.0 : 0.0, 0.0);
+        const int entry = (int)((i / c.volume) % 9);
+        links[c.offset + i] = make_double2((entry == 0 || entry == 4 || entry == 8) ? 1.0 : 0.0, 0.0);
     }
 }
 
@@ -276,9 +279,14 @@ static int grid_for(int64_t n, int threads) {
 }
 
 cudaError_t launch_su3_identity(ym_ensemble *e) {
-    for (int64_t ch = 0; ch < e->n_chains; ++ch) {
-        const ChainInfo &c = e->chains[ch];
-        k_su3_identity<<<grid_for(36 * c.volume, 256), 256, 0, e->stream>>>(e->d_links, c.offset, c.volume);
+    int64_t vmax = 0;
+    for (const ChainInfo &c : e->chains) vmax = c.volume > vmax ? c.volume : vmax;
+    // one launch per 65,535 chains (the grid's y limit)
+    for (int64_t first = 0; first < e->n_chains; first += 65535) {
+        const int64_t count = e->n_chains - first < 65535 ? e->n_chains - first : 65535;
+        const int64_t bx = (grid_for(36 * vmax, 256) + count - 1) / count;   // about grid_for's total
+        k_su3_identity<<<dim3((unsigned)(bx < 1 ? 1 : bx), (unsigned)count), 256, 0, e->stream>>>(
+            e->d_chains + first, e->d_links);
     }
     return cudaGetLastError();
 }

@@ -91,6 +91,7 @@ SIGNATURES = {
     "ym_su3_spatial_stout_smear": [VP, VP, f64, i64, i32],
     "ym_su3_spatial_stride2_block": [VP, VP],
     "ym_su3_glueball_measure": [VP, VP, P(GlueballPlan), P(f64), P(f64), P(f64), P(f64)],
+    "ym_su3_glueball_prepare": [VP, VP, P(GlueballPlan)],
     "ym_periodic_connected_estimator": [P(f64), i64, i64, P(f64), P(f64), P(f64)],
     "ym_connected_from_samples": [P(f64), i64, i64, i64, P(f64)],
     "ym_jackknife_replicas": [P(f64), i64, i64, P(f64)],

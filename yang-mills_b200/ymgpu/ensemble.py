@@ -467,6 +467,23 @@ class Ensemble:
         check(lib().ym_su3_spatial_stout_smear(self._h, dst.handle, float(rho), int(levels),
                                                int(lift_level_cap)), "spatial_stout_smear")
 
+    @staticmethod
+    def _glueball_plan(levels, rho, blocked):
+        lv = np.ascontiguousarray(np.asarray(levels, dtype=np.int64))
+        blocked = list(blocked)
+        fine = (C.c_void_p * max(1, len(blocked)))(*[b[0].handle.value for b in blocked])
+        coarse = (C.c_void_p * max(1, len(blocked)))(*[b[1].handle.value for b in blocked])
+        first = np.ascontiguousarray(np.asarray([b[2] for b in blocked] or [0], dtype=np.int64))
+        plan = GlueballPlan(float(rho), len(lv), _i64p(lv), len(blocked), fine, coarse, _i64p(first))
+        return plan, (lv, fine, coarse, first)       # the arrays the plan points into
+
+    def glueball_prepare(self, smeared: "Ensemble", levels, rho: float = 0.1, blocked=()) -> None:
+        """Build and upload the measurement graph of glueball_measure with
+        these arguments without measuring (ym_su3_glueball_prepare)."""
+        plan, keep = self._glueball_plan(levels, rho, blocked)
+        check(lib().ym_su3_glueball_prepare(self._h, smeared.handle, C.byref(plan)), "glueball_prepare")
+        del keep
+
     def glueball_measure(self, smeared: "Ensemble", levels, rho: float = 0.1, blocked=()):
         """One glueball measurement as one captured graph (ym_su3_glueball_measure):
         this handle's links smeared in place in `smeared` through the
@@ -475,12 +492,8 @@ class Ensemble:
         first_chain.. of `smeared` blocked into `coarse` and measured.
         Returns (plaquette, rectangle, blocked_plaquette, blocked_rectangle),
         each [level, slice]."""
-        lv = np.ascontiguousarray(np.asarray(levels, dtype=np.int64))
         blocked = list(blocked)
-        fine = (C.c_void_p * max(1, len(blocked)))(*[b[0].handle.value for b in blocked])
-        coarse = (C.c_void_p * max(1, len(blocked)))(*[b[1].handle.value for b in blocked])
-        first = np.ascontiguousarray(np.asarray([b[2] for b in blocked] or [0], dtype=np.int64))
-        plan = GlueballPlan(float(rho), len(lv), _i64p(lv), len(blocked), fine, coarse, _i64p(first))
+        plan, (lv, fine, coarse, first) = self._glueball_plan(levels, rho, blocked)
         n_sl = sum(e[3] for e in smeared.extents)
         n_bl = sum(sum(e[3] for e in b[1].extents) for b in blocked)
         p = np.zeros((len(lv), n_sl), np.float64)

@@ -214,6 +214,7 @@ class GlueballPipelineResult:
     surfaces: List[SurfaceResult] = field(default_factory=list)
     sweep_seconds: float = 0.0
     measure_seconds: float = 0.0
+    prepare_seconds: float = 0.0      # building the measurement graph, once
     link_updates: int = 0
     sweep_layout: dict = field(default_factory=dict)   # the handle tuner's choice
     sweep_path: str = ""
@@ -240,6 +241,7 @@ def scalar_glueball_pipeline(groups: Sequence[Tuple[int, Sequence[int]]] = ((128
     seeds = [derive_su3_chain_seed(master_seed, i) for i in range(len(extents))]
     res = GlueballPipelineResult()
     samples: Dict[Tuple[int, int, bool], List[Tuple[np.ndarray, np.ndarray]]] = {}
+    # chains are listed group by group, so each group's chains are consecutive
     with Ensemble(extents, beta, seeds, lift_reference_caps=True, device=device) as ens:
         per_group = [[i for i, g in enumerate(group_of) if g == gi] for gi in range(len(groups))]
         # Scratch handles made once and refilled every measurement: the
@@ -259,7 +261,13 @@ def scalar_glueball_pipeline(groups: Sequence[Tuple[int, Sequence[int]]] = ((128
         for gi in blocked_groups:
             blocked_at[gi] = k
             k += sum(extents[c][3] for c in per_group[gi])
+        levels_sorted = sorted(stout_levels)
+        plan_blocked = [(subs[gi], coarse[gi], per_group[gi][0]) for gi in blocked_groups]
         try:
+            # the measurement graph, built once before the first measurement
+            t0 = time.perf_counter()
+            ens.glueball_prepare(sm, levels_sorted, rho, plan_blocked)
+            res.prepare_seconds = time.perf_counter() - t0
             t0 = time.perf_counter()
             ens.metropolis_sweeps(proposal_angle, thermalization)
             ens.synchronize()
@@ -276,29 +284,31 @@ def scalar_glueball_pipeline(groups: Sequence[Tuple[int, Sequence[int]]] = ((128
                 # count (0, 5, 10 costs 10 levels, not 15; the same links as
                 # smearing from scratch), operators after each count, the
                 # blockable groups blocked and measured
-                levels_sorted = sorted(stout_levels)
-                plaq, rect, bplaq, brect = ens.glueball_measure(
-                    sm, levels_sorted, rho, [(subs[gi], coarse[gi], per_group[gi][0]) for gi in blocked_groups])
+                plaq, rect, bplaq, brect = ens.glueball_measure(sm, levels_sorted, rho, plan_blocked)
+                # a group's chains are consecutive, so its time slices form one
+                # (chains, N3) block of every output row
                 for li, levels in enumerate(levels_sorted):
                     for gi, chains in enumerate(per_group):
-                        samples.setdefault((gi, levels, False), []).extend(
-                            (plaq[li, slice_at[c]:slice_at[c] + extents[c][3]].copy(),
-                             rect[li, slice_at[c]:slice_at[c] + extents[c][3]].copy()) for c in chains)
+                        nt, a = extents[chains[0]][3], slice_at[chains[0]]
+                        n = len(chains) * nt
+                        samples.setdefault((gi, levels, False), []).append(
+                            (plaq[li, a:a + n].reshape(len(chains), nt).copy(),
+                             rect[li, a:a + n].reshape(len(chains), nt).copy()))
                         if gi in subs:
                             k0 = blocked_at[gi]
-                            samples.setdefault((gi, levels, True), []).extend(
-                                (bplaq[li, k0 + j * extents[c][3]:k0 + (j + 1) * extents[c][3]].copy(),
-                                 brect[li, k0 + j * extents[c][3]:k0 + (j + 1) * extents[c][3]].copy())
-                                for j, c in enumerate(chains))
+                            samples.setdefault((gi, levels, True), []).append(
+                                (bplaq[li, k0:k0 + n].reshape(len(chains), nt).copy(),
+                                 brect[li, k0:k0 + n].reshape(len(chains), nt).copy()))
                 res.measure_seconds += time.perf_counter() - t1
         finally:
             for h in list(coarse.values()) + list(subs.values()) + [sm]:
                 h.close()
         res.link_updates = int(sum(np.prod(e) * 4 for e in extents)) * (
             thermalization + measurements * sweeps_between_measurements)
-    for (gi, levels, blocked), rows in sorted(samples.items()):
-        p = np.stack([r[0] for r in rows])
-        r = np.stack([r[1] for r in rows])
+    for (gi, levels, blocked), blocks in sorted(samples.items()):
+        # rows: measurement by measurement, chains in order within each
+        p = np.concatenate([blk[0] for blk in blocks])
+        r = np.concatenate([blk[1] for blk in blocks])
         nt = p.shape[1]
         reps = G.jackknife_replicas(p)
         end = min(4, nt // 2)
