@@ -664,26 +664,65 @@ def main():
 
     configs_extra = other_configs()
 
-    # end to end through the C ABI with host buffers: upload the lattice from
-    # pinned host memory, sweep, measure, download the lattice
-    host = torch.empty(links * 18, dtype=torch.float64, pin_memory=True)
-    host_np = host.numpy().view(np.complex128).reshape(links, 3, 3)
-    ens.download(0, host_np)
-    e2e_steps = max(3, min(args.steps, 20))
+    # end to end through the C ABI with host buffers: every step uploads a
+    # lattice from pinned host memory in the reference layout, sweeps it,
+    # measures its plaquette and downloads it.  Two independent lattices
+    # (two handles, two host buffers, one host thread each, the ctypes calls
+    # releasing the interpreter lock) take turns, so one lattice's download
+    # overlaps the other's upload on the full-duplex host link; each thread's
+    # steps depend on its own previous download.  Also the same steps on one
+    # lattice alone (every transfer serialised).
+    import threading
+    e2e_steps = max(4, min(args.steps, 20)) // 2 * 2
+    lattices = [ens, ens.like()]
+    ens.copy_to(lattices[1])
+    lattices[1].sweep_index = ens.sweep_index + 1000
+    hosts = []
+    for h in lattices:
+        buf = torch.empty(links * 18, dtype=torch.float64, pin_memory=True)
+        hosts.append(buf.numpy().view(np.complex128).reshape(links, 3, 3))
+        h.download(0, hosts[-1])
+
+    def e2e_step(h, host_np):
+        h.upload(0, host_np)
+        h.metropolis_sweeps(ANGLE, 1)
+        h.average_plaquette()
+        h.download(0, host_np)
+
+    def e2e_worker(i, n, gate):
+        gate.wait()
+        for _ in range(n):
+            e2e_step(lattices[i], hosts[i])
+
+    gate = threading.Barrier(3)
+    workers = [threading.Thread(target=e2e_worker, args=(i, e2e_steps // 2, gate)) for i in range(2)]
+    for w in workers:
+        w.start()
     barrier()
+    gate.wait()
     t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        ens.upload(0, host_np)
-        ens.metropolis_sweeps(ANGLE, 1)
-        ens.average_plaquette()
-        ens.download(0, host_np)
+    for w in workers:
+        w.join()
     t1 = time.perf_counter()
     e2e_s = max_over_ranks(t1 - t0)
+    barrier()
+    t2 = time.perf_counter()
+    for _ in range(e2e_steps // 2):
+        e2e_step(ens, hosts[0])
+    t3 = time.perf_counter()
+    e2e_one_s = max_over_ranks(t3 - t2)
     e2e = {"value": world * links * e2e_steps / e2e_s, "unit": UNIT,
            "h2d_bytes_per_step": links * LINK_BYTES,
            "d2h_bytes_per_step": links * LINK_BYTES + 8,
+           "steps": e2e_steps,
            "path": "ym_ensemble_upload -> ym_su3_metropolis_sweeps -> ym_average_plaquette "
-                   "-> ym_ensemble_download (pinned host lattice in the reference layout)"}
+                   "-> ym_ensemble_download (pinned host lattice in the reference layout), two "
+                   "independent lattices on two host threads taking turns",
+           "one_lattice": {"value": world * links * (e2e_steps // 2) / e2e_one_s, "unit": UNIT,
+                           "steps": e2e_steps // 2,
+                           "note": "the same steps on one lattice: upload, sweep, plaquette and "
+                                   "download strictly in turn"}}
+    lattices[1].close()
     ens.close()
 
     if rank == 0:

@@ -373,6 +373,18 @@ __device__ __forceinline__ double retr_col64(const cf *x, cf c0, cf c1, cf c2) {
 
 __device__ __forceinline__ cf csel(bool p, cf a, cf b) { return cf{p ? a.re : b.re, p ? a.im : b.im}; }
 
+// cos h and sin h by Horner's rule in y = h^2 (Taylor coefficients through
+// h^14 / h^15: for |h| <= 1.45, the largest argument the lifted half width
+// 2.5 gives, the next term is below 2e-9), binary32 fused multiply-adds.
+__device__ __forceinline__ void cos_sin_f(float h, float &c, float &s) {
+    const float y = h * h;
+    c = fmaf(fmaf(fmaf(fmaf(fmaf(fmaf(fmaf(-1.f / 87178291200.f, y, 1.f / 479001600.f), y, -1.f / 3628800.f), y,
+                                 1.f / 40320.f), y, -1.f / 720.f), y, 1.f / 24.f), y, -0.5f), y, 1.f);
+    s = h * fmaf(fmaf(fmaf(fmaf(fmaf(fmaf(fmaf(-1.f / 1307674368000.f, y, 1.f / 6227020800.f), y,
+                                          -1.f / 39916800.f), y, 1.f / 362880.f), y, -1.f / 5040.f), y,
+                           1.f / 120.f), y, -1.f / 6.f), y, 1.f);
+}
+
 // One hit of a generator chosen per thread, without divergent control
 // flow.  exp(i theta T^g) acts on rows (i, j) as the 2x2 matrix
 // [[r00, r01], [r10, r11]] and multiplies the remaining row k by ek:
@@ -387,9 +399,9 @@ __device__ __forceinline__ void hit_any_f(m3f &u, const m3f &a, double rr[3], do
                                           unsigned &accepted) {
     const bool diag = g == 7;
     float s1, c1;
-    sincosf(diag ? theta * 0.28867513459481287f : 0.5f * theta, &s1, &c1);
+    cos_sin_f(diag ? theta * 0.28867513459481287f : 0.5f * theta, c1, s1);
     // e^{-2 i phi} of lambda_8 from the same pair by the double-angle
-    // identities (one sincosf per hit instead of two)
+    // identities (one cos/sin pair per hit instead of two)
     const float c2 = fmaf(c1, c1, -s1 * s1), s2 = -2.f * s1 * c1;
     const int kind = diag ? 3 : ((g == 2) ? 2 : ((g == 1 || g == 4 || g == 6) ? 1 : 0));
     const cf zero = cfm(0.f, 0.f);
@@ -442,6 +454,43 @@ __device__ __forceinline__ void hit_any_f(m3f &u, const m3f &a, double rr[3], do
     accepted += acc ? 1u : 0u;
 }
 
+// The reference's eight ordered hits, unrolled: every hit's generator is a
+// compile-time constant (no branches), and the link-independent work of
+// later hits (stream words, angle, rotation entries) is free to overlap the
+// current hit's dependent chain.
+__device__ __forceinline__ unsigned visit_ordered_f(m3f &u, const m3f &a, double beta3, double angle,
+                                                    uint64_t key) {
+    double rr[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) rr[i] = retr_row64(u.e[i], a, i);
+    double old_tr = (rr[0] + rr[1]) + rr[2];
+    unsigned accepted = 0;
+#pragma unroll
+    for (int h = 0; h < 8; ++h) {
+        const uint64_t w_angle = splitmix_at(key, (uint64_t)(2 * h));
+        const uint64_t w_acc = splitmix_at(key, (uint64_t)(2 * h + 1));
+        const float theta = (float)grid_angle(w_angle, angle);
+        const double unif = unit_from(w_acc);
+        if (h == 7) {
+            float s1, c1, s2, c2;
+            cos_sin_f(theta * 0.28867513459481287f, c1, s1);
+            cos_sin_f(theta * -0.57735026918962573f, c2, s2);
+            hit_diag_f(u, a, rr, old_tr, cfm(c1, s1), cfm(c2, s2), beta3, unif, accepted);
+        } else {
+            float s, c;
+            cos_sin_f(0.5f * theta, c, s);
+            const int kind = (h == 2) ? 2 : ((h == 1 || h == 4 || h == 6) ? 1 : 0);
+            if (h <= 2)
+                hit_block_f<0, 1>(u, a, rr, old_tr, kind, c, s, beta3, unif, accepted);
+            else if (h <= 4)
+                hit_block_f<0, 2>(u, a, rr, old_tr, kind, c, s, beta3, unif, accepted);
+            else
+                hit_block_f<1, 2>(u, a, rr, old_tr, kind, c, s, beta3, unif, accepted);
+        }
+    }
+    return accepted;
+}
+
 // exp(i theta T^a) in closed form: c = cos(theta/2), s = sin(theta/2) for
 // the SU(2) subgroups; diag(e^{i theta/(2 sqrt3)} x2, e^{-i theta/sqrt3}).
 // Ordered generators take the specialised per-generator code (every thread
@@ -449,44 +498,18 @@ __device__ __forceinline__ void hit_any_f(m3f &u, const m3f &a, double rr[3], do
 // converged hit_any_f.
 __device__ __forceinline__ unsigned visit_f(m3f &u, const m3f &a, double beta3, double angle,
                                             uint64_t key, int uniform) {
+    if (!uniform) return visit_ordered_f(u, a, beta3, angle, key);
     double rr[3];
 #pragma unroll
     for (int i = 0; i < 3; ++i) rr[i] = retr_row64(u.e[i], a, i);
     double old_tr = (rr[0] + rr[1]) + rr[2];
     unsigned accepted = 0;
-    if (uniform) {
-#pragma unroll 1
-        for (int h = 0; h < 8; ++h) {
-            const uint64_t w_angle = splitmix_at(key, (uint64_t)(2 * h));
-            const uint64_t w_acc = splitmix_at(key, (uint64_t)(2 * h + 1));
-            hit_any_f(u, a, rr, old_tr, (int)((w_angle >> 52) & 7),
-                      (float)grid_angle(w_angle, angle), beta3, unit_from(w_acc), accepted);
-        }
-        return accepted;
-    }
 #pragma unroll 1
     for (int h = 0; h < 8; ++h) {
         const uint64_t w_angle = splitmix_at(key, (uint64_t)(2 * h));
         const uint64_t w_acc = splitmix_at(key, (uint64_t)(2 * h + 1));
-        const int g = h;
-        const float theta = (float)grid_angle(w_angle, angle);
-        const double unif = unit_from(w_acc);
-        if (g == 7) {
-            float s1, c1, s2, c2;
-            sincosf(theta * 0.28867513459481287f, &s1, &c1);
-            sincosf(theta * -0.57735026918962573f, &s2, &c2);
-            hit_diag_f(u, a, rr, old_tr, cfm(c1, s1), cfm(c2, s2), beta3, unif, accepted);
-        } else {
-            float s, c;
-            sincosf(0.5f * theta, &s, &c);
-            const int kind = (g == 2) ? 2 : ((g == 1 || g == 4 || g == 6) ? 1 : 0);
-            if (g <= 2)
-                hit_block_f<0, 1>(u, a, rr, old_tr, kind, c, s, beta3, unif, accepted);
-            else if (g <= 4)
-                hit_block_f<0, 2>(u, a, rr, old_tr, kind, c, s, beta3, unif, accepted);
-            else
-                hit_block_f<1, 2>(u, a, rr, old_tr, kind, c, s, beta3, unif, accepted);
-        }
+        hit_any_f(u, a, rr, old_tr, (int)((w_angle >> 52) & 7),
+                  (float)grid_angle(w_angle, angle), beta3, unit_from(w_acc), accepted);
     }
     return accepted;
 }
