@@ -10,6 +10,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -32,6 +33,82 @@ int32_t cuda_status(cudaError_t err) {
 
 int32_t ym::record_cuda_status(cudaError_t err) { return cuda_status(err); }
 
+// ---- device memory -----------------------------------------------------
+// Every device buffer of the library comes from the device's stream-ordered
+// memory pool, allocated and freed on one allocation stream per device, with
+// the pool's release threshold raised so that freed blocks stay in the pool
+// for the next handle instead of going back to the driver.  Plain
+// cudaMalloc / cudaFree on these machines take milliseconds each and, about
+// one call in forty, 50 to 180 ms, which a batch of short campaigns (each
+// creating and destroying handles) would otherwise pay many times.
+// dev_alloc synchronises the allocation stream, so a block is ready for any
+// stream when it returns; dev_free first waits for the device to go idle, as
+// cudaFree does, so no kernel in flight on any stream still reads the block.
+// The pool keeps what it holds until the process exits; an allocation that
+// finds the device full gives the pool's idle blocks back and tries once
+// more.
+namespace {
+
+struct DevicePool {
+    std::mutex lock;
+    cudaStream_t stream[64] = {};
+};
+
+DevicePool &device_pool() {
+    static DevicePool p;
+    return p;
+}
+
+cudaError_t alloc_stream(int dev, cudaStream_t *out) {
+    DevicePool &p = device_pool();
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> g(p.lock);
+    if (!p.stream[dev]) {
+        cudaMemPool_t pool = nullptr;
+        cudaError_t err = cudaDeviceGetDefaultMemPool(&pool, dev);
+        uint64_t keep = UINT64_MAX;
+        if (err == cudaSuccess) err = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        if (err == cudaSuccess) err = cudaStreamCreateWithFlags(&p.stream[dev], cudaStreamNonBlocking);
+        if (err != cudaSuccess) return err;
+    }
+    *out = p.stream[dev];
+    return cudaSuccess;
+}
+
+}  // namespace
+
+cudaError_t ym::dev_alloc(void **ptr, size_t bytes) {
+    int dev = 0;
+    cudaError_t err = cudaGetDevice(&dev);
+    cudaStream_t s = nullptr;
+    if (err == cudaSuccess) err = alloc_stream(dev, &s);
+    if (err == cudaSuccess) {
+        err = cudaMallocAsync(ptr, bytes, s);
+        if (err == cudaErrorMemoryAllocation) {
+            cudaGetLastError();
+            cudaMemPool_t pool = nullptr;
+            if (cudaStreamSynchronize(s) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess &&
+                cudaMemPoolTrimTo(pool, 0) == cudaSuccess)
+                err = cudaMallocAsync(ptr, bytes, s);
+        }
+    }
+    if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+    return err;
+}
+
+void ym::dev_free(void *ptr) {
+    if (!ptr) return;
+    cudaPointerAttributes at{};
+    cudaStream_t s = nullptr;
+    if (cudaPointerGetAttributes(&at, ptr) != cudaSuccess || alloc_stream(at.device, &s) != cudaSuccess) return;
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != at.device) cudaSetDevice(at.device);
+    cudaDeviceSynchronize();
+    cudaFreeAsync(ptr, s);
+    if (cur != at.device) cudaSetDevice(cur);
+}
+
 namespace {
 
 #define YM_CUDA(call)                                 \
@@ -51,7 +128,7 @@ constexpr int kGraphSweeps = 8;                      // sweeps per captured grap
 
 template <class T>
 cudaError_t dalloc(T **p, size_t count) {
-    return cudaMalloc(reinterpret_cast<void **>(p), count * sizeof(T) + 16);
+    return ym::dev_alloc(reinterpret_cast<void **>(p), count * sizeof(T) + 16);
 }
 
 void free_all(ym_ensemble *e) {
@@ -59,12 +136,12 @@ void free_all(ym_ensemble *e) {
     if (e->measure_graph) cudaGraphExecDestroy(e->measure_graph);
     if (e->run_graph) cudaGraphExecDestroy(e->run_graph);
     if (e->glueball_graph) cudaGraphExecDestroy(e->glueball_graph);
-    if (e->d_gb_series) cudaFree(e->d_gb_series);
-    if (e->d_series) cudaFree(e->d_series);
-    if (e->d_wilson_series) cudaFree(e->d_wilson_series);
-    if (e->d_poly_series) cudaFree(e->d_poly_series);
-    if (e->d_loop_row) cudaFree(e->d_loop_row);
-    if (e->d_series_row) cudaFree(e->d_series_row);
+    if (e->d_gb_series) ym::dev_free(e->d_gb_series);
+    if (e->d_series) ym::dev_free(e->d_series);
+    if (e->d_wilson_series) ym::dev_free(e->d_wilson_series);
+    if (e->d_poly_series) ym::dev_free(e->d_poly_series);
+    if (e->d_loop_row) ym::dev_free(e->d_loop_row);
+    if (e->d_series_row) ym::dev_free(e->d_series_row);
     for (auto &pool : e->events)
         for (auto &p : pool) {
             cudaEventDestroy(p.start);
@@ -77,9 +154,9 @@ void free_all(ym_ensemble *e) {
                     e->d_slice_chain, e->d_slice_t, e->d_slice_plaq, e->d_slice_rect,
                     e->d_links_tmp, e->d_query_error, e->d_query, e->d_steps, e->d_terms};
     for (void *p : ptrs)
-        if (p) cudaFree(p);
+        if (p) ym::dev_free(p);
     for (auto &l : e->layouts)
-        if (l.d_items) cudaFree(l.d_items);
+        if (l.d_items) ym::dev_free(l.d_items);
     if (e->stream) cudaStreamDestroy(e->stream);
 }
 
@@ -666,7 +743,7 @@ static cudaError_t ensure_series(ym_ensemble *e, int64_t n_measurements) {
         if (e->measure_graph) cudaGraphExecDestroy(e->measure_graph);
         e->measure_graph = nullptr;
         drop_run_graph(e);
-        if (e->d_series) cudaFree(e->d_series);
+        if (e->d_series) ym::dev_free(e->d_series);
         e->d_series = nullptr;
         e->series_capacity = 0;
         cudaError_t err = dalloc(&e->d_series, (size_t)(n_measurements * e->n_chains));
@@ -768,8 +845,8 @@ int32_t ym_su3_measured_sweeps(ym_ensemble *e, double angle, int32_t generator_m
 static cudaError_t ensure_loop_series(ym_ensemble *e, int64_t rows) {
     if (e->loop_capacity < rows) {
         drop_run_graph(e);
-        if (e->d_wilson_series) cudaFree(e->d_wilson_series);
-        if (e->d_poly_series) cudaFree(e->d_poly_series);
+        if (e->d_wilson_series) ym::dev_free(e->d_wilson_series);
+        if (e->d_poly_series) ym::dev_free(e->d_poly_series);
         e->d_wilson_series = nullptr;
         e->d_poly_series = nullptr;
         e->loop_capacity = 0;
@@ -1339,7 +1416,7 @@ static int32_t glueball_graph(ym_ensemble *ens, ym_ensemble *sm, const ym_glueba
     if (sm->gb_series_capacity < need) {
         if (sm->glueball_graph) cudaGraphExecDestroy(sm->glueball_graph);
         sm->glueball_graph = nullptr;
-        if (sm->d_gb_series) cudaFree(sm->d_gb_series);
+        if (sm->d_gb_series) ym::dev_free(sm->d_gb_series);
         sm->d_gb_series = nullptr;
         sm->gb_series_capacity = 0;
         YM_CUDA(dalloc(&sm->d_gb_series, (size_t)need));
@@ -1622,7 +1699,7 @@ void free_model(ym_proposal_model *m) {
     void *ptrs[] = {m->d_params, m->d_adam_m, m->d_adam_v, m->d_image, m->d_error, m->d_feat,
                     m->d_mrec, m->d_b3, m->d_y, m->d_partial, m->d_groups, m->d_grad, m->d_objective};
     for (void *p : ptrs)
-        if (p) cudaFree(p);
+        if (p) ym::dev_free(p);
     if (m->stream) cudaStreamDestroy(m->stream);
 }
 
@@ -1634,7 +1711,7 @@ cudaError_t ensure_rows(ym_proposal_model *m, int64_t rows) {
     float **bufs[] = {&m->d_feat, &m->d_mrec, &m->d_b3, &m->d_y};
     for (float **b : bufs)
         if (*b) {
-            cudaFree(*b);
+            ym::dev_free(*b);
             *b = nullptr;
         }
     m->row_capacity = 0;
@@ -1648,8 +1725,8 @@ cudaError_t ensure_rows(ym_proposal_model *m, int64_t rows) {
 
 cudaError_t ensure_partials(ym_proposal_model *m, int64_t tiles) {
     if (tiles <= m->partial_capacity) return cudaSuccess;
-    if (m->d_partial) cudaFree(m->d_partial);
-    if (m->d_groups) cudaFree(m->d_groups);
+    if (m->d_partial) ym::dev_free(m->d_partial);
+    if (m->d_groups) ym::dev_free(m->d_groups);
     m->d_partial = nullptr;
     m->d_groups = nullptr;
     m->partial_capacity = 0;
@@ -1662,7 +1739,7 @@ cudaError_t ensure_partials(ym_proposal_model *m, int64_t tiles) {
 
 cudaError_t ensure_objectives(ym_proposal_model *m, int64_t n) {
     if (n <= m->objective_capacity) return cudaSuccess;
-    if (m->d_objective) cudaFree(m->d_objective);
+    if (m->d_objective) ym::dev_free(m->d_objective);
     m->d_objective = nullptr;
     m->objective_capacity = 0;
     cudaError_t err = dalloc(&m->d_objective, (size_t)n);
@@ -1753,7 +1830,7 @@ int32_t ym_device_wait_selftest(int32_t device, int64_t limit_ns) {
     cudaError_t err = cudaMemset(d_err, 0, sizeof(unsigned));
     if (err == cudaSuccess) err = ym::launch_lp_wait_selftest((uint64_t)limit_ns, d_err, nullptr);
     if (err == cudaSuccess) err = cudaMemcpy(&bits, d_err, sizeof bits, cudaMemcpyDeviceToHost);
-    cudaFree(d_err);
+    ym::dev_free(d_err);
     YM_CUDA(err);
     return bits ? YM_ERR_DEVICE_WAIT_TIMEOUT : YM_OK;
 }
@@ -1892,9 +1969,9 @@ int32_t ym_learned_records(ym_ensemble *e, int32_t parity, int32_t mu, float *fe
     if (err == cudaSuccess)
         err = cudaMemcpyAsync(hm.data(), d_m, hm.size() * sizeof(float), cudaMemcpyDeviceToHost, e->stream);
     if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);
-    cudaFree(d_f);
-    cudaFree(d_m);
-    cudaFree(d_b);
+    ym::dev_free(d_f);
+    ym::dev_free(d_m);
+    ym::dev_free(d_b);
     YM_CUDA(err);
     // tiles are laid out chain by chain, 128 sites of the parity each
     int64_t tile0 = 0, out = 0;

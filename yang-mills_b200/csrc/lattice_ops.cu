@@ -559,29 +559,29 @@ constexpr int64_t kQueryDoubles = 64;
 
 cudaError_t ensure_query(ym_ensemble *e) {
     cudaError_t err = cudaSuccess;
-    if (!e->d_query_error) err = cudaMalloc(reinterpret_cast<void **>(&e->d_query_error), 16);
+    if (!e->d_query_error) err = ym::dev_alloc(reinterpret_cast<void **>(&e->d_query_error), 16);
     if (err == cudaSuccess && !e->d_query)
-        err = cudaMalloc(reinterpret_cast<void **>(&e->d_query), kQueryDoubles * sizeof(double));
+        err = ym::dev_alloc(reinterpret_cast<void **>(&e->d_query), kQueryDoubles * sizeof(double));
     if (err == cudaSuccess) err = cudaMemsetAsync(e->d_query_error, 0, sizeof(unsigned), e->stream);
     return err;
 }
 
 cudaError_t ensure_steps(ym_ensemble *e, int64_t n) {
     if (e->steps_capacity >= n) return cudaSuccess;
-    if (e->d_steps) cudaFree(e->d_steps);
+    if (e->d_steps) ym::dev_free(e->d_steps);
     e->d_steps = nullptr;
     e->steps_capacity = 0;
-    cudaError_t err = cudaMalloc(reinterpret_cast<void **>(&e->d_steps), (size_t)n * sizeof(int32_t));
+    cudaError_t err = ym::dev_alloc(reinterpret_cast<void **>(&e->d_steps), (size_t)n * sizeof(int32_t));
     if (err == cudaSuccess) e->steps_capacity = n;
     return err;
 }
 
 cudaError_t ensure_terms(ym_ensemble *e, int64_t n) {
     if (e->terms_capacity >= n) return cudaSuccess;
-    if (e->d_terms) cudaFree(e->d_terms);
+    if (e->d_terms) ym::dev_free(e->d_terms);
     e->d_terms = nullptr;
     e->terms_capacity = 0;
-    cudaError_t err = cudaMalloc(reinterpret_cast<void **>(&e->d_terms), (size_t)n * sizeof(double));
+    cudaError_t err = ym::dev_alloc(reinterpret_cast<void **>(&e->d_terms), (size_t)n * sizeof(double));
     if (err == cudaSuccess) e->terms_capacity = n;
     return err;
 }

@@ -189,6 +189,11 @@ cudaError_t launch_lp_wait_selftest(uint64_t limit_ns, unsigned *err, cudaStream
 cudaError_t launch_su3_identity(ym_ensemble *e);
 cudaError_t launch_su3_from_aos(ym_ensemble *e, int64_t chain);
 cudaError_t launch_su3_to_aos(ym_ensemble *e, int64_t chain);
+// Device memory of the library (capi.cu): from the current device's
+// stream-ordered pool, ready for every stream on return; dev_free gives a
+// block back to the pool of the device that holds it.
+cudaError_t dev_alloc(void **ptr, size_t bytes);
+void dev_free(void *ptr);
 cudaError_t launch_su3_metropolis(ym_ensemble *e, int parity, int mu, double angle, int uniform);
 // The same sub-sweep in the fast form (su3_metropolis_fast.cu);
 // launch_su3_metropolis dispatches to it when e->fast_sweeps is set.
