@@ -388,9 +388,10 @@ int32_t ym_su3_spatial_stride2_block(ym_ensemble *src, ym_ensemble *dst);
 /* One measurement of the scalar-glueball production cadence
  * (glueball_scalar_production.rs:257-381, per retained configuration): the
  * links of `ens` copied into `smeared` (same extents), then for each stout
- * level count in `levels` (ascending; 0 allowed) the levels smeared in place
+ * level count in `levels` (ascending; 0 allowed) the levels smeared
  * continuing from the previous count (sequential levels, so the same links
- * as smearing from scratch; spatial_stout_smear glueball_smearing.rs:257),
+ * as smearing from scratch; spatial_stout_smear glueball_smearing.rs:257;
+ * on return `smeared` holds the last level),
  * scalar_a1pp_operator_basis of every chain (glueball_operators.rs:93-160),
  * and for every blocked group g the chains first_chain[g].. of `smeared`
  * copied into fine[g], spatial_stride2_block into coarse[g]

@@ -1432,29 +1432,23 @@ static int32_t glueball_graph(ym_ensemble *ens, ym_ensemble *sm, const ym_glueba
         cudaStream_t s0 = sm->stream;
         cudaError_t err = cudaMemcpyAsync(sm->d_links, ens->d_links, (size_t)sm->total_elems * sizeof(double2),
                                           cudaMemcpyDeviceToDevice, s0);
+        // levels continue from the previous count, ping-ponging between the
+        // handle's links and its second buffer; `cur` holds the latest level
+        // (each level from the previous one, so the same links as smearing
+        // from scratch), and the operators and group copies read it there
+        double2 *cur = sm->d_links;
         int64_t done = 0;
         for (int32_t i = 0; i < plan->n_levels && err == cudaSuccess; ++i) {
-            // levels continue from the previous count, in place (the
-            // ping-pong of ym_su3_spatial_stout_smear with src == dst)
-            const int64_t n = plan->levels[i] - done;
-            if (n > 0) {
-                const double2 *in = sm->d_links;
-                if (n % 2 == 1) {
-                    err = cudaMemcpyAsync(sm->d_links_tmp, sm->d_links, (size_t)sm->total_elems * sizeof(double2),
-                                          cudaMemcpyDeviceToDevice, s0);
-                    in = sm->d_links_tmp;
-                }
-                for (int64_t k = 1; k <= n && err == cudaSuccess; ++k) {
-                    double2 *out = ((n - k) % 2 == 0) ? sm->d_links : sm->d_links_tmp;
-                    err = ym::launch_stout_level(sm, in, out, plan->rho);
-                    in = out;
-                }
-                done = plan->levels[i];
+            for (int64_t k = done; k < plan->levels[i] && err == cudaSuccess; ++k) {
+                double2 *out = cur == sm->d_links ? sm->d_links_tmp : sm->d_links;
+                err = ym::launch_stout_level(sm, cur, out, plan->rho);
+                cur = out;
             }
+            done = plan->levels[i] > done ? plan->levels[i] : done;
             double *row = sm->d_gb_series + per_level * i;
             if (err == cudaSuccess)
                 err = ym::launch_operator_basis(sm, sm->d_site_vals, sm->d_slice_chain, sm->d_slice_t,
-                                                sm->n_slices, sm->d_slice_plaq, sm->d_slice_rect);
+                                                sm->n_slices, sm->d_slice_plaq, sm->d_slice_rect, cur);
             if (err == cudaSuccess)
                 err = cudaMemcpyAsync(row, sm->d_slice_plaq, (size_t)sm->n_slices * sizeof(double),
                                       cudaMemcpyDeviceToDevice, s0);
@@ -1467,7 +1461,7 @@ static int32_t glueball_graph(ym_ensemble *ens, ym_ensemble *sm, const ym_glueba
                 const ChainInfo &a = sm->chains[plan->first_chain[g]];
                 const ChainInfo &z = sm->chains[plan->first_chain[g] + f->n_chains - 1];
                 const size_t bytes = (size_t)(z.offset - a.offset + z.volume * 36) * sizeof(double2);
-                err = cudaMemcpyAsync(f->d_links, sm->d_links + a.offset, bytes, cudaMemcpyDeviceToDevice, s0);
+                err = cudaMemcpyAsync(f->d_links, cur + a.offset, bytes, cudaMemcpyDeviceToDevice, s0);
                 if (err == cudaSuccess) err = ym::launch_block(f, c);
                 if (err == cudaSuccess)
                     err = ym::launch_operator_basis(c, c->d_site_vals, c->d_slice_chain, c->d_slice_t, c->n_slices,
@@ -1481,6 +1475,11 @@ static int32_t glueball_graph(ym_ensemble *ens, ym_ensemble *sm, const ym_glueba
                 brow += c->n_slices;
             }
         }
+        // the last level ends in the handle's own links (a copy only when
+        // the total level count is odd)
+        if (err == cudaSuccess && cur != sm->d_links)
+            err = cudaMemcpyAsync(sm->d_links, cur, (size_t)sm->total_elems * sizeof(double2),
+                                  cudaMemcpyDeviceToDevice, s0);
         return err;
     };
     if (!sm->glueball_graph || sm->glueball_key != key || sm->glueball_rho != plan->rho) {

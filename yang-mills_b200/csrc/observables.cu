@@ -417,9 +417,9 @@ cudaError_t launch_polyakov(ym_ensemble *e, int dir, double *d_partial, double *
 
 cudaError_t launch_operator_basis(ym_ensemble *e, double2 *d_site_vals, const int32_t *d_slice_chain,
                                   const int32_t *d_slice_t, int64_t n_slices, double *d_plaq,
-                                  double *d_rect) {
+                                  double *d_rect, const double2 *links) {
     k_operator_sites<<<(unsigned)e->n_site_tiles, T, 0, e->stream>>>(e->d_chains, e->d_site_tiles,
-                                                                    e->d_links, d_site_vals);
+                                                                    links ? links : e->d_links, d_site_vals);
     k_operator_reduce<<<(unsigned)n_slices, 256, 0, e->stream>>>(e->d_chains, d_slice_chain, d_slice_t,
                                                                 d_site_vals, d_plaq, d_rect);
     return cudaGetLastError();

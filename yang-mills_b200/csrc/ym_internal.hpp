@@ -220,9 +220,11 @@ cudaError_t launch_store_rows(cudaStream_t st, const double *src, int64_t n, dou
 // observables.cu / smear.cu
 cudaError_t launch_wilson_loops(ym_ensemble *e, int rmax, int tmax, double *d_partial, double *d_out);
 cudaError_t launch_polyakov(ym_ensemble *e, int dir, double *d_partial, double *d_out);
+// The operator basis of e's links, or of `links` (a buffer in e's layout)
+// when given.
 cudaError_t launch_operator_basis(ym_ensemble *e, double2 *d_site_vals, const int32_t *d_slice_chain,
                                   const int32_t *d_slice_t, int64_t n_slices, double *d_plaq,
-                                  double *d_rect);
+                                  double *d_rect, const double2 *links = nullptr);
 cudaError_t launch_stout_level(ym_ensemble *e, const double2 *in, double2 *out, double rho);
 cudaError_t launch_block(ym_ensemble *fine, ym_ensemble *coarse);
 // Per-chain means of tile partials [tile][width] (loops: / volume; dir >= 0:
