@@ -78,6 +78,14 @@ int32_t ym_ensemble_create(const ym_ensemble_desc *desc, ym_ensemble **out);
 int32_t ym_ensemble_destroy(ym_ensemble *ens);
 int32_t ym_ensemble_info(const ym_ensemble *ens, int64_t *n_chains, int64_t *total_links,
                          int32_t *group, int32_t *precision);
+/* Device memory (no reference counterpart): handles draw their device
+ * buffers from the device's default stream-ordered memory pool, and what a
+ * destroyed handle frees stays in that pool for the next handle (creating
+ * and destroying handles then costs well under a millisecond).  Other code
+ * in the process that allocates with cudaMalloc sees the pooled memory as
+ * taken; this call gives the pool's unused memory on `device` back to the
+ * driver, after waiting for the device to go idle. */
+int32_t ym_device_release_pooled_memory(int32_t device);
 /* Cold start: every link the identity (all chains). */
 int32_t ym_ensemble_set_identity(ym_ensemble *ens);
 /* Hot start (no reference counterpart: the reference always starts cold,

@@ -354,6 +354,18 @@ extern "C" {
 
 int32_t ym_last_cuda_error(void) { return g_last_cuda_error; }
 
+int32_t ym_device_release_pooled_memory(int32_t device) {
+    int count = 0;
+    YM_CUDA(cudaGetDeviceCount(&count));
+    if (device < 0 || device >= count) return YM_ERR_INVALID_ARGUMENT;
+    YM_CUDA(cudaSetDevice(device));
+    YM_CUDA(cudaDeviceSynchronize());
+    cudaMemPool_t pool = nullptr;
+    YM_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+    YM_CUDA(cudaMemPoolTrimTo(pool, 0));
+    return YM_OK;
+}
+
 int32_t ym_ensemble_create(const ym_ensemble_desc *desc, ym_ensemble **out) {
     if (!desc || !out || !desc->extents || !desc->beta || !desc->chain_seed) return YM_ERR_NULL_ARGUMENT;
     *out = nullptr;

@@ -14,6 +14,14 @@ from .learned import ProposalModel
 from .lattice import Lattice4
 from .su3_lattice import Su3Lattice4
 
+
+def release_pooled_memory(device: int = 0) -> None:
+    """Give the device memory that destroyed handles left in the device's
+    memory pool back to the driver (ym_device_release_pooled_memory)."""
+    from .errors import check
+    check(lib().ym_device_release_pooled_memory(int(device)), "release_pooled_memory")
+
+
 __all__ = ["Ensemble", "Lattice4", "Su3Lattice4", "path_holonomy", "YmError", "lib", "LIB_PATH", "su2_ensemble",
            "su3_ensemble", "su3_lattice", "glueball", "SU2", "SU3", "F64", "F32_TWO_ROW", "ORDERED",
-           "UNIFORM", "learned", "ProposalModel"]
+           "UNIFORM", "learned", "ProposalModel", "release_pooled_memory"]

@@ -108,6 +108,7 @@ SIGNATURES = {
     "ym_model_create": [i32, u64, f64, P(VP)],
     "ym_model_destroy": [VP],
     "ym_device_wait_selftest": [i32, i64],
+    "ym_device_release_pooled_memory": [i32],
     "ym_model_get_params": [VP, P(C.c_float)],
     "ym_model_set_params": [VP, P(C.c_float)],
     "ym_model_forward": [VP, P(C.c_float), i64, P(C.c_float)],
