@@ -560,11 +560,8 @@ def main():
         e2.set_identity()
         e2.markov_sweeps(200, 3, sampler="kennedy-pendleton")
         e2.synchronize()
-        series = np.zeros(500)
         t = time.perf_counter()
-        for i in range(500):
-            e2.markov_sweeps(1, 3, sampler="kennedy-pendleton")
-            series[i] = e2.average_plaquette()[0]
+        series = e2.su2_measured_sweeps(500, 1, 3, sampler="kennedy-pendleton")[:, 0]
         secs = time.perf_counter() - t
         # per-launch device time of the two update kernels (one launch = one
         # parity and direction: 5,000 links), 20 more sweeps under the events
@@ -580,9 +577,10 @@ def main():
             "plaquette_mean": float(series.mean()), "plaquette_ess_per_s": world * d2.effective_sample_size / secs,
             "heatbath_us_per_launch": 1e3 * hb_ms / max(1, hb_n),
             "overrelax_us_per_launch": 1e3 * or_ms / max(1, or_n),
-            "note": "200 + 500 sweeps from a cold start, plaquette every sweep (read back each sweep); "
-                    "per-launch times from 20 further sweeps under CUDA events (1.28 MB lattice, "
-                    "L2-resident: absolute rates, not an HBM fraction)"}
+            "note": "200 + 500 sweeps from a cold start, plaquette every sweep into a device series "
+                    "(ym_su2_measured_sweeps: one captured graph per measurement, one read-back at "
+                    "the end); per-launch times from 20 further sweeps under CUDA events (1.28 MB "
+                    "lattice, L2-resident: absolute rates, not an HBM fraction)"}
         # SU(3) 64 x 4^4 beta=6.0 FP64, generator uniform in 1..8, half width 0.3
         seeds = [derive_su3_chain_seed(MASTER_SEED, rank * 64 + i) for i in range(64)]
         e1 = ymgpu.Ensemble([[4, 4, 4, 4]] * 64, BETA, seeds, device=local)

@@ -224,6 +224,17 @@ int32_t ym_su3_reference_average_plaquette(ym_ensemble *ens, double *per_chain);
 enum { YM_SU2_SAMPLER_REFERENCE = 0, YM_SU2_SAMPLER_KENNEDY_PENDLETON = 1 };
 int32_t ym_su2_markov_sweeps(ym_ensemble *ens, int64_t max_attempts_per_link,
                              int64_t overrelaxation_sweeps, int32_t sampler, int64_t n_sweeps);
+/* The SU(2) run_chain cadence (su2_ensemble.rs:465-486: sweeps, then the
+ * average plaquette, per measurement) without a host round trip per
+ * measurement: n_measurements times {sweeps_per_measurement sweeps of
+ * ym_su2_markov_sweeps, average plaquette of every chain}, replayed from one
+ * captured CUDA graph; series[m * n_chains + chain] receives measurement m.
+ * The same links, streams and values as the separate calls; an exhausted
+ * attempt limit anywhere in the run returns
+ * YM_ERR_HEATBATH_ATTEMPT_LIMIT_EXCEEDED after it. */
+int32_t ym_su2_measured_sweeps(ym_ensemble *ens, int64_t max_attempts_per_link, int64_t overrelaxation_sweeps,
+                               int32_t sampler, int64_t n_measurements, int64_t sweeps_per_measurement,
+                               double *series);
 /* overrelaxation_sweep (su2_ensemble.rs:344-346), checkerboard order. */
 int32_t ym_su2_overrelaxation_sweeps(ym_ensemble *ens, int64_t n_sweeps);
 /* Heat-bath proposals (attempts) and updates per chain since creation or

@@ -145,3 +145,31 @@ def test_published_su2_plaquette(sampler):
     pooled, err = means.mean(), means.std(ddof=1) / np.sqrt(nch)
     published, published_err = 0.6022919679191184, 0.0004173286094490
     assert abs(pooled - published) <= 4.0 * np.hypot(err, published_err)
+
+
+@pytest.mark.parametrize("sampler", ["reference", "kennedy-pendleton"])
+def test_measured_sweeps_equal_separate_calls(sampler):
+    """ym_su2_measured_sweeps (one captured graph per measurement) gives the
+    series, links and attempt counts of markov_sweeps + average_plaquette
+    called one measurement at a time, bit for bit; a later call continues
+    the same chain; the attempt limit still fails closed."""
+    import ymgpu
+    from ymgpu.errors import YmError
+    exts = [[4, 4, 4, 6], [6, 4, 4, 4]]
+    with ymgpu.Ensemble(exts, 2.3, [21, 22], group=ymgpu.SU2) as a, \
+            ymgpu.Ensemble(exts, 2.3, [21, 22], group=ymgpu.SU2) as b:
+        got = np.concatenate([a.su2_measured_sweeps(5, 2, 3, sampler=sampler),
+                              a.su2_measured_sweeps(4, 2, 3, sampler=sampler)])
+        want = []
+        for _ in range(9):
+            b.markov_sweeps(2, 3, sampler=sampler)
+            want.append(b.average_plaquette())
+        assert np.array_equal(got, np.array(want))
+        for ch in range(2):
+            assert np.array_equal(a.download(ch), b.download(ch))
+        pa, ua = a.heatbath_accounting()
+        pb, ub = b.heatbath_accounting()
+        assert np.array_equal(pa, pb) and np.array_equal(ua, ub)
+        with pytest.raises(YmError) as e:
+            a.su2_measured_sweeps(2, 1, 0, max_attempts_per_link=1, sampler=sampler)
+        assert e.value.variant == "HeatbathAttemptLimitExceeded"

@@ -136,6 +136,7 @@ void free_all(ym_ensemble *e) {
     if (e->measure_graph) cudaGraphExecDestroy(e->measure_graph);
     if (e->run_graph) cudaGraphExecDestroy(e->run_graph);
     if (e->glueball_graph) cudaGraphExecDestroy(e->glueball_graph);
+    if (e->su2_graph) cudaGraphExecDestroy(e->su2_graph);
     if (e->d_gb_series) ym::dev_free(e->d_gb_series);
     if (e->d_series) ym::dev_free(e->d_series);
     if (e->d_wilson_series) ym::dev_free(e->d_wilson_series);
@@ -754,6 +755,8 @@ static cudaError_t ensure_series(ym_ensemble *e, int64_t n_measurements) {
     if (e->series_capacity < n_measurements) {
         if (e->measure_graph) cudaGraphExecDestroy(e->measure_graph);
         e->measure_graph = nullptr;
+        if (e->su2_graph) cudaGraphExecDestroy(e->su2_graph);
+        e->su2_graph = nullptr;
         drop_run_graph(e);
         if (e->d_series) ym::dev_free(e->d_series);
         e->d_series = nullptr;
@@ -1634,6 +1637,71 @@ int32_t ym_su2_markov_sweeps(ym_ensemble *e, int64_t max_attempts_per_link,
     for (int64_t ch = 0; ch < e->n_chains; ++ch)
         e->proposals[ch] += (uint64_t)n_sweeps * 4u * (uint64_t)e->chains[ch].volume;
     return take_device_error(e);
+}
+
+int32_t ym_su2_measured_sweeps(ym_ensemble *e, int64_t max_attempts_per_link, int64_t overrelaxation_sweeps,
+                               int32_t sampler, int64_t n_measurements, int64_t sweeps_per_measurement,
+                               double *series) {
+    if (!e || (!series && n_measurements > 0)) return YM_ERR_NULL_ARGUMENT;
+    if (e->group != YM_GROUP_SU2) return YM_ERR_WRONG_GROUP;
+    for (const ChainInfo &c : e->chains)
+        if (!std::isfinite(c.beta) || c.beta < 0.0 || c.beta > kMaxSu2Beta)
+            return YM_ERR_BETA_OUTSIDE_REFERENCE_RANGE;
+    if (max_attempts_per_link == 0) return YM_ERR_ZERO_HEATBATH_ATTEMPT_LIMIT;
+    if (max_attempts_per_link < 0 || max_attempts_per_link > (int64_t(1) << 30) || overrelaxation_sweeps < 0 ||
+        n_measurements < 0 || sweeps_per_measurement < 0 ||
+        (sampler != YM_SU2_SAMPLER_REFERENCE && sampler != YM_SU2_SAMPLER_KENNEDY_PENDLETON))
+        return YM_ERR_INVALID_ARGUMENT;
+    int32_t st = require_checkerboard(e);
+    if (st) return st;
+    st = set_device(e);
+    if (st) return st;
+    if (n_measurements == 0) return YM_OK;
+    YM_CUDA(ensure_series(e, n_measurements));
+    YM_CUDA(cudaMemsetAsync(e->d_series_row, 0, sizeof(uint64_t), e->stream));
+    // one measurement: the sweeps of ym_su2_markov_sweeps, then the average
+    // plaquette of every chain into the next row of the device series
+    auto step = [&]() -> cudaError_t {
+        cudaError_t err = cudaSuccess;
+        for (int64_t k = 0; k < sweeps_per_measurement && err == cudaSuccess; ++k) {
+            for (int parity = 0; parity < 2 && err == cudaSuccess; ++parity)
+                for (int mu = 0; mu < 4 && err == cudaSuccess; ++mu)
+                    err = ym::launch_su2_heatbath(e, parity, mu, (int)max_attempts_per_link, sampler);
+            if (err == cudaSuccess) err = ym::launch_advance_sweep(e);
+            for (int64_t o = 0; o < overrelaxation_sweeps && err == cudaSuccess; ++o)
+                for (int parity = 0; parity < 2 && err == cudaSuccess; ++parity)
+                    for (int mu = 0; mu < 4 && err == cudaSuccess; ++mu) err = ym::launch_su2_overrelax(e, parity, mu);
+        }
+        if (err == cudaSuccess) err = ym::launch_su2_plaquette_partials(e);
+        if (err == cudaSuccess) err = ym::launch_chain_reduce(e, e->d_partial, e->d_result, 0, 6.0);
+        if (err == cudaSuccess) err = ym::launch_store_series(e, e->d_series, e->d_series_row);
+        return err;
+    };
+    const int64_t key[4] = {max_attempts_per_link, overrelaxation_sweeps, sampler, sweeps_per_measurement};
+    if (!e->su2_graph || !std::equal(key, key + 4, e->su2_graph_key)) {
+        if (e->su2_graph) cudaGraphExecDestroy(e->su2_graph);
+        e->su2_graph = nullptr;
+        cudaGraph_t g = nullptr;
+        YM_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+        cudaError_t err = step();
+        const cudaError_t end = cudaStreamEndCapture(e->stream, &g);
+        if (err == cudaSuccess) err = end;
+        if (err == cudaSuccess) err = cudaGraphInstantiate(&e->su2_graph, g, 0);
+        if (g) cudaGraphDestroy(g);
+        YM_CUDA(err);
+        std::copy(key, key + 4, e->su2_graph_key);
+    }
+    for (int64_t m = 0; m < n_measurements; ++m) YM_CUDA(cudaGraphLaunch(e->su2_graph, e->stream));
+    YM_CUDA(cudaMemcpyAsync(series, e->d_series, (size_t)(n_measurements * e->n_chains) * sizeof(double),
+                            cudaMemcpyDeviceToHost, e->stream));
+    YM_CUDA(cudaStreamSynchronize(e->stream));
+    for (int64_t ch = 0; ch < e->n_chains; ++ch)
+        e->proposals[ch] += (uint64_t)(n_measurements * sweeps_per_measurement) * 4u * (uint64_t)e->chains[ch].volume;
+    st = take_device_error(e);
+    if (st) return st;
+    for (int64_t k = 0; k < n_measurements * e->n_chains; ++k)
+        if (!std::isfinite(series[k])) return YM_ERR_NON_FINITE_STATISTIC;
+    return YM_OK;
 }
 
 int32_t ym_su2_overrelaxation_sweeps(ym_ensemble *e, int64_t n_sweeps) {

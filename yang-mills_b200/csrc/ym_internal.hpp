@@ -101,6 +101,10 @@ struct ym_ensemble {
     double measure_graph_angle = 0.0;
     int32_t measure_graph_mode = -1;
     int64_t measure_graph_stride = -1;
+    // SU(2) measurement graph (ym_su2_measured_sweeps) and what it was made
+    // for: attempt limit, overrelaxation sweeps, sampler, sweeps per row.
+    cudaGraphExec_t su2_graph = nullptr;
+    int64_t su2_graph_key[4] = {-1, -1, -1, -1};
     // Small-chain path choice: -1 not yet measured, 0 tiled launches, 1 the
     // chain-resident kernel (picked by timing both on the first sweeps).
     int32_t resident_choice = -1;

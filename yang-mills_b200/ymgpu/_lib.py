@@ -99,6 +99,7 @@ SIGNATURES = {
     "ym_su3_reunitarize": [VP],
     "ym_ensemble_convert": [VP, VP],
     "ym_su2_markov_sweeps": [VP, i64, i64, i32, i64],
+    "ym_su2_measured_sweeps": [VP, i64, i64, i32, i64, i64, P(f64)],
     "ym_su2_overrelaxation_sweeps": [VP, i64],
     "ym_su2_accounting": [VP, P(u64), P(u64)],
     "ym_su2_max_unit_residual": [VP, P(f64)],

@@ -246,6 +246,19 @@ class Ensemble:
                                          int(overrelaxation_sweeps), code, int(n_sweeps)),
               "su2_markov_sweeps")
 
+    def su2_measured_sweeps(self, n_measurements: int, sweeps_per_measurement: int = 1,
+                            overrelaxation_sweeps: int = 1, max_attempts_per_link: int = 10000,
+                            sampler: str = "reference") -> np.ndarray:
+        """run_chain's cadence on the device: n_measurements times
+        {sweeps_per_measurement markov_sweeps, average plaquette}, one
+        captured graph; returns the series [measurement, chain]."""
+        code = {"reference": 0, "kennedy-pendleton": 1}[sampler]
+        out = np.zeros((int(n_measurements), self.n_chains), np.float64)
+        check(lib().ym_su2_measured_sweeps(self._h, int(max_attempts_per_link), int(overrelaxation_sweeps), code,
+                                           int(n_measurements), int(sweeps_per_measurement), _f64p(out)),
+              "su2_measured_sweeps")
+        return out
+
     def overrelaxation_sweeps(self, n_sweeps: int = 1) -> None:
         check(lib().ym_su2_overrelaxation_sweeps(self._h, int(n_sweeps)), "su2_overrelaxation")
 
