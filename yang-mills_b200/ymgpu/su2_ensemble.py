@@ -175,10 +175,9 @@ def run_chains(configs, sampler: str = "reference", device: int = 0):
                    group=SU2, device=device)
     try:
         ens.markov_sweeps(therm, n_or, attempts, sampler)
-        meas = np.zeros((len(configs), nmeas))
-        for m in range(nmeas):
-            ens.markov_sweeps(stride, n_or, attempts, sampler)
-            meas[:, m] = ens.average_plaquette()
+        # measurement m after `stride` more sweeps, all on the device
+        # (ym_su2_measured_sweeps: the values of the separate calls)
+        meas = ens.su2_measured_sweeps(nmeas, stride, n_or, attempts, sampler).T.copy()
         prop, upd = ens.heatbath_accounting()
         res = ens.max_unit_residual()
     finally:
