@@ -161,10 +161,9 @@ def run_chains(configs: List[Su3EnsembleConfig], lift_reference_caps: bool = Fal
                    lift_reference_caps=lift_reference_caps, device=device)
     try:
         ens.metropolis_sweeps(angle, therm, generator_mode)
-        meas = np.zeros((len(configs), nmeas))
-        for m in range(nmeas):
-            ens.metropolis_sweeps(angle, stride, generator_mode)
-            meas[:, m] = ens.average_plaquette()
+        # measurement m after `stride` more sweeps, all on the device
+        # (ym_su3_measured_sweeps: the values of the separate calls)
+        meas = ens.measured_sweeps(angle, nmeas, stride, generator_mode).T.copy()
         if np.any(meas < -0.5 - PLAQUETTE_TOLERANCE) or np.any(meas > 1.0 + PLAQUETTE_TOLERANCE):
             raise _err("NonFiniteStatistic", "run_chain")
         prop, acc = ens.accounting()
