@@ -356,14 +356,19 @@ extern "C" {
 int32_t ym_last_cuda_error(void) { return g_last_cuda_error; }
 
 int32_t ym_device_release_pooled_memory(int32_t device) {
-    int count = 0;
+    int count = 0, current = 0;
     YM_CUDA(cudaGetDeviceCount(&count));
     if (device < 0 || device >= count) return YM_ERR_INVALID_ARGUMENT;
-    YM_CUDA(cudaSetDevice(device));
-    YM_CUDA(cudaDeviceSynchronize());
+    YM_CUDA(cudaGetDevice(&current));
+    // the caller's current device is restored whatever happens
+    cudaError_t err = cudaSetDevice(device);
+    if (err == cudaSuccess) err = cudaDeviceSynchronize();
     cudaMemPool_t pool = nullptr;
-    YM_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
-    YM_CUDA(cudaMemPoolTrimTo(pool, 0));
+    if (err == cudaSuccess) err = cudaDeviceGetDefaultMemPool(&pool, device);
+    if (err == cudaSuccess) err = cudaMemPoolTrimTo(pool, 0);
+    const cudaError_t back = cudaSetDevice(current);
+    YM_CUDA(err);
+    YM_CUDA(back);
     return YM_OK;
 }
 
