@@ -173,3 +173,22 @@ def test_measured_sweeps_equal_separate_calls(sampler):
         with pytest.raises(YmError) as e:
             a.su2_measured_sweeps(2, 1, 0, max_attempts_per_link=1, sampler=sampler)
         assert e.value.variant == "HeatbathAttemptLimitExceeded"
+
+
+def test_measured_sweeps_edge_cases():
+    """No measurements is a no-op; an SU(3) handle is the wrong group; a zero
+    attempt limit and a negative count are refused before any launch."""
+    import ymgpu
+    from ymgpu.errors import YmError
+    with ymgpu.Ensemble([[4, 4, 4, 4]], 2.3, 5, group=ymgpu.SU2) as ens:
+        before = ens.download(0)
+        assert ens.su2_measured_sweeps(0).shape == (0, 1)
+        assert np.array_equal(before, ens.download(0))
+        with pytest.raises(YmError) as e:
+            ens.su2_measured_sweeps(1, max_attempts_per_link=0)
+        assert e.value.variant == "ZeroHeatbathAttemptLimit"
+        assert ymgpu.lib().ym_su2_measured_sweeps(ens.handle, 100, 1, 0, -1, 1, None) != 0
+    with ymgpu.Ensemble([[4, 4, 4, 4]], 6.0, 5) as su3:
+        with pytest.raises(YmError) as e:
+            su3.su2_measured_sweeps(1)
+        assert e.value.variant == "WrongGroup"
