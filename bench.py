@@ -57,6 +57,7 @@ LOOP_EVERY = 10                       # sweeps between Wilson / Polyakov measure
 FAST_CHECK_SWEEPS = 10                # sweeps per form when the fast form is compared with the exact one
 MASTER_SEED = 0x2C02198105010002
 LINK_BYTES = 144                      # FP64 3x3 complex
+E2E_LATTICES = 3                      # independent lattices in flight end to end (upload, sweep, download)
 LINKS_PER_UPDATE = 9                  # 8 link reads + 1 write per checkerboard update
 FALLBACK_HBM_GBS = 6650.0
 
@@ -664,17 +665,18 @@ def main():
 
     # end to end through the C ABI with host buffers: every step uploads a
     # lattice from pinned host memory in the reference layout, sweeps it,
-    # measures its plaquette and downloads it.  Two independent lattices
-    # (two handles, two host buffers, one host thread each, the ctypes calls
-    # releasing the interpreter lock) take turns, so one lattice's download
-    # overlaps the other's upload on the full-duplex host link; each thread's
-    # steps depend on its own previous download.  Also the same steps on one
-    # lattice alone (every transfer serialised).
+    # measures its plaquette and downloads it.  E2E_LATTICES independent
+    # lattices (one handle, one host buffer and one host thread each, the
+    # ctypes calls releasing the interpreter lock) take turns, so while one
+    # lattice uploads another downloads on the full-duplex host link and a
+    # third sweeps; each thread's steps depend on its own previous download.
+    # Also the same steps on one lattice alone (every transfer serialised).
     import threading
-    e2e_steps = max(4, min(args.steps, 20)) // 2 * 2
-    lattices = [ens, ens.like()]
-    ens.copy_to(lattices[1])
-    lattices[1].sweep_index = ens.sweep_index + 1000
+    e2e_steps = max(2 * E2E_LATTICES, min(args.steps, 10 * E2E_LATTICES)) // E2E_LATTICES * E2E_LATTICES
+    lattices = [ens] + [ens.like() for _ in range(E2E_LATTICES - 1)]
+    for i, h in enumerate(lattices[1:], 1):
+        ens.copy_to(h)
+        h.sweep_index = ens.sweep_index + 1000 * i
     hosts = []
     for h in lattices:
         buf = torch.empty(links * 18, dtype=torch.float64, pin_memory=True)
@@ -692,8 +694,9 @@ def main():
         for _ in range(n):
             e2e_step(lattices[i], hosts[i])
 
-    gate = threading.Barrier(3)
-    workers = [threading.Thread(target=e2e_worker, args=(i, e2e_steps // 2, gate)) for i in range(2)]
+    gate = threading.Barrier(E2E_LATTICES + 1)
+    workers = [threading.Thread(target=e2e_worker, args=(i, e2e_steps // E2E_LATTICES, gate))
+               for i in range(E2E_LATTICES)]
     for w in workers:
         w.start()
     barrier()
@@ -705,7 +708,7 @@ def main():
     e2e_s = max_over_ranks(t1 - t0)
     barrier()
     t2 = time.perf_counter()
-    for _ in range(e2e_steps // 2):
+    for _ in range(e2e_steps // E2E_LATTICES):
         e2e_step(ens, hosts[0])
     t3 = time.perf_counter()
     e2e_one_s = max_over_ranks(t3 - t2)
@@ -714,13 +717,14 @@ def main():
            "d2h_bytes_per_step": links * LINK_BYTES + 8,
            "steps": e2e_steps,
            "path": "ym_ensemble_upload -> ym_su3_metropolis_sweeps -> ym_average_plaquette "
-                   "-> ym_ensemble_download (pinned host lattice in the reference layout), two "
-                   "independent lattices on two host threads taking turns",
-           "one_lattice": {"value": world * links * (e2e_steps // 2) / e2e_one_s, "unit": UNIT,
-                           "steps": e2e_steps // 2,
+                   f"-> ym_ensemble_download (pinned host lattice in the reference layout), {E2E_LATTICES} "
+                   f"independent lattices on {E2E_LATTICES} host threads taking turns",
+           "one_lattice": {"value": world * links * (e2e_steps // E2E_LATTICES) / e2e_one_s, "unit": UNIT,
+                           "steps": e2e_steps // E2E_LATTICES,
                            "note": "the same steps on one lattice: upload, sweep, plaquette and "
                                    "download strictly in turn"}}
-    lattices[1].close()
+    for h in lattices[1:]:
+        h.close()
     ens.close()
 
     if rank == 0:
