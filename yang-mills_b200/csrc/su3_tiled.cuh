@@ -331,8 +331,8 @@ __device__ __forceinline__ void hit_block_drawn(m3 &u, const double2 (*sa)[T], d
 // Fast form only (YM_TILED_FAST): cos h and sin h as polynomials in
 // y = h^2 by Horner's rule with fused multiply-adds, the Taylor coefficients
 // 1/k! truncated where the next term is below 1e-19 for the half widths
-// served: through h^14 / h^15 for K = 13 (|h| <= 0.173), through h^18 /
-// h^19 for K = 16 (|h| <= 0.578).
+// served: through h^14 / h^15 for K <= 13 (|h| <= 0.173), through h^18 /
+// h^19 above (|h| <= 0.578).
 template <int K>
 __device__ __forceinline__ void cos_sin_horner(double h, double &c, double &s) {
     constexpr int NT = K <= 13 ? 7 : 9;
@@ -422,8 +422,13 @@ __device__ __forceinline__ unsigned visit(m3 &u, const double2 (*sa)[T], double 
 //     K is taken from the proposal half width a so that every admissible
 //     angle stops within K terms: |t_k| <= |h|^k / k! with |h| <= a/2 for
 //     generators 1..7 and |h| <= 0.5774 a (at most 0.5 after lambda8's
-//     halving) for generator 8; a <= 0.3 stops by k = 13 (0.1732^13/13! =
-//     2e-20), a <= 1 by k = 16 (0.5^16/16! = 7e-19).
+//     halving) for generator 8.  Terms the reference still adds past K
+//     must be too small to move their sum (below half an ulp of it): for
+//     a <= 0.3, K = 11 (t_12 <= 0.1732^12/12! = 1.5e-18 against sums near
+//     0.985, t_13 / s <= 0.1732^12/13! = 1.2e-19); for a <= 1, K = 14
+//     (t_15 / s <= 0.5^14/15! = 4.7e-17 < 2^-54, t_16 <= 7.3e-19), so the
+//     sums are the reference's bit for bit (checked on the CPU against
+//     the loop run to the cutoff over millions of grid angles).
 //   * the decision is accept_step's u < exp(-max(dS, 0)) (for m = 0,
 //     exp(-0) = 1 > u, as its explicit branch gives); the accepted rows are
 //     selected, not branched to.
@@ -837,10 +842,10 @@ cudaError_t tiled_launch(ym_ensemble *e, int parity, int mu, double angle, int u
     if (configured_device != dev) {
         const void *drawn[4] = {(const void *)k_su3_metropolis<0>, (const void *)k_su3_metropolis<1>,
                                 (const void *)k_su3_metropolis<2>, (const void *)k_su3_metropolis<3>};
-        const void *ordered[8] = {(const void *)k_su3_metropolis_ring<0, 13>, (const void *)k_su3_metropolis_ring<1, 13>,
-                                  (const void *)k_su3_metropolis_ring<2, 13>, (const void *)k_su3_metropolis_ring<3, 13>,
-                                  (const void *)k_su3_metropolis_ring<0, 16>, (const void *)k_su3_metropolis_ring<1, 16>,
-                                  (const void *)k_su3_metropolis_ring<2, 16>, (const void *)k_su3_metropolis_ring<3, 16>};
+        const void *ordered[8] = {(const void *)k_su3_metropolis_ring<0, 11>, (const void *)k_su3_metropolis_ring<1, 11>,
+                                  (const void *)k_su3_metropolis_ring<2, 11>, (const void *)k_su3_metropolis_ring<3, 11>,
+                                  (const void *)k_su3_metropolis_ring<0, 14>, (const void *)k_su3_metropolis_ring<1, 14>,
+                                  (const void *)k_su3_metropolis_ring<2, 14>, (const void *)k_su3_metropolis_ring<3, 14>};
         for (const void *f : drawn)
             if (cudaError_t err = set_smem(f, kStageBytes)) return err;
         for (const void *f : ordered)
@@ -848,8 +853,8 @@ cudaError_t tiled_launch(ym_ensemble *e, int parity, int mu, double angle, int u
         configured_device = dev;
     }
     if (uniform) metro_launch_drawn(e, parity, mu, angle);
-    else if (angle <= 0.3) metro_launch_ordered<13>(e, parity, mu, angle);
-    else metro_launch_ordered<16>(e, parity, mu, angle);
+    else if (angle <= 0.3) metro_launch_ordered<11>(e, parity, mu, angle);
+    else metro_launch_ordered<14>(e, parity, mu, angle);
     return cudaGetLastError();
 }
 
