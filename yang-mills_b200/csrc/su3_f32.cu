@@ -35,10 +35,11 @@ template <int MU>
 __global__ void __launch_bounds__(T, YM_F32_MIN_BLOCKS)
 k_f32_metropolis(const ChainInfo *__restrict__ chains, const Tile *__restrict__ tiles,
                  float2 *__restrict__ links, int parity, double angle, int uniform,
-                 const uint64_t *__restrict__ sweep_ptr, unsigned long long *__restrict__ accepts) {
+                 const uint64_t *__restrict__ sweep_ptr, unsigned long long *__restrict__ accepts,
+                 int reverse) {
     __shared__ __align__(16) float2 stage[18][T];   // 18 KB: three staged factors
     const StageF<T> bufs{stage, stage + 6, stage + 12};
-    const Tile tile = tiles[blockIdx.x];
+    const Tile tile = tiles[reverse ? gridDim.x - 1 - blockIdx.x : blockIdx.x];
     const ChainInfo c = chains[tile.chain];
     const int64_t t = tile.start + threadIdx.x;
     const uint64_t sweep = *sweep_ptr;
@@ -235,11 +236,14 @@ float2 *f32_links(ym_ensemble *e) { return reinterpret_cast<float2 *>(e->d_links
 cudaError_t launch_f32_metropolis(ym_ensemble *e, int parity, int mu, double angle, int uniform) {
     const dim3 g((unsigned)e->n_half_tiles), b(T);
     float2 *l = f32_links(e);
+    // consecutive sub-sweeps in opposite tile orders (each starts on the
+    // links the previous one left in L2; the order changes no bit)
+    const int reverse = (parity * 4 + mu) & 1;
     switch (mu) {
-    case 0: k_f32_metropolis<0><<<g, b, 0, e->stream>>>(e->d_chains, e->d_half_tiles, l, parity, angle, uniform, e->d_sweep, e->d_accepts); break;
-    case 1: k_f32_metropolis<1><<<g, b, 0, e->stream>>>(e->d_chains, e->d_half_tiles, l, parity, angle, uniform, e->d_sweep, e->d_accepts); break;
-    case 2: k_f32_metropolis<2><<<g, b, 0, e->stream>>>(e->d_chains, e->d_half_tiles, l, parity, angle, uniform, e->d_sweep, e->d_accepts); break;
-    default: k_f32_metropolis<3><<<g, b, 0, e->stream>>>(e->d_chains, e->d_half_tiles, l, parity, angle, uniform, e->d_sweep, e->d_accepts); break;
+    case 0: k_f32_metropolis<0><<<g, b, 0, e->stream>>>(e->d_chains, e->d_half_tiles, l, parity, angle, uniform, e->d_sweep, e->d_accepts, reverse); break;
+    case 1: k_f32_metropolis<1><<<g, b, 0, e->stream>>>(e->d_chains, e->d_half_tiles, l, parity, angle, uniform, e->d_sweep, e->d_accepts, reverse); break;
+    case 2: k_f32_metropolis<2><<<g, b, 0, e->stream>>>(e->d_chains, e->d_half_tiles, l, parity, angle, uniform, e->d_sweep, e->d_accepts, reverse); break;
+    default: k_f32_metropolis<3><<<g, b, 0, e->stream>>>(e->d_chains, e->d_half_tiles, l, parity, angle, uniform, e->d_sweep, e->d_accepts, reverse); break;
     }
     return cudaGetLastError();
 }

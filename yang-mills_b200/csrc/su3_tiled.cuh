@@ -633,7 +633,7 @@ __global__ void __launch_bounds__(T, YM_METRO_MIN_BLOCKS)
 k_su3_metropolis(const ChainInfo *__restrict__ chains, const Tile *__restrict__ tiles,
                  double2 *__restrict__ links, int parity, double angle, int uniform,
                  const uint64_t *__restrict__ sweep_ptr, unsigned long long *__restrict__ accepts,
-                 int log2_item) {
+                 int log2_item, int reverse) {
     __shared__ double2 sa[9][T];
     extern __shared__ __align__(16) double2 stage_mem[];
     const StageBufs bufs{reinterpret_cast<double2 (*)[T]>(stage_mem),
@@ -641,7 +641,8 @@ k_su3_metropolis(const ChainInfo *__restrict__ chains, const Tile *__restrict__ 
                          reinterpret_cast<double2 (*)[T]>(stage_mem + 18 * T)};
     // The CTA takes T >> log2_item work items of 2^log2_item sites each
     // (possibly of different chains); padding items have chain < 0.
-    const Tile tile = tiles[(int64_t)blockIdx.x * (T >> log2_item) + (threadIdx.x >> log2_item)];
+    const int64_t cta = reverse ? (int64_t)gridDim.x - 1 - blockIdx.x : (int64_t)blockIdx.x;
+    const Tile tile = tiles[cta * (T >> log2_item) + (threadIdx.x >> log2_item)];
     const bool live = tile.chain >= 0;
     const ChainInfo c = chains[live ? tile.chain : 0];
     const int64_t t = tile.start + (threadIdx.x & ((1u << log2_item) - 1u));
@@ -762,11 +763,12 @@ __global__ void __launch_bounds__(T, 2)
 k_su3_metropolis_ring(const ChainInfo *__restrict__ chains, const Tile *__restrict__ tiles,
                       double2 *__restrict__ links, int parity, double angle,
                       const uint64_t *__restrict__ sweep_ptr, unsigned long long *__restrict__ accepts,
-                      int log2_item) {
+                      int log2_item, int reverse) {
     extern __shared__ __align__(16) double2 ring_mem[];
     auto buf = [&](int i) { return reinterpret_cast<double2 (*)[T]>(ring_mem + (size_t)i * 9 * T); };
     const TermSet s0{{buf(0), buf(1), buf(2)}}, s1{{buf(3), buf(4), buf(5)}};
-    const Tile tile = tiles[(int64_t)blockIdx.x * (T >> log2_item) + (threadIdx.x >> log2_item)];
+    const int64_t cta = reverse ? (int64_t)gridDim.x - 1 - blockIdx.x : (int64_t)blockIdx.x;
+    const Tile tile = tiles[cta * (T >> log2_item) + (threadIdx.x >> log2_item)];
     const bool live = tile.chain >= 0;
     const ChainInfo c = chains[live ? tile.chain : 0];
     const int64_t t = tile.start + (threadIdx.x & ((1u << log2_item) - 1u));
@@ -801,27 +803,27 @@ constexpr size_t kRingBytes = (size_t)kRingBuffers * 9 * T * sizeof(double2);
 // sites, chain order or by descending chain volume (all layouts give the
 // same bits).
 template <int K>
-void metro_launch_ordered(ym_ensemble *e, int parity, int mu, double angle) {
+void metro_launch_ordered(ym_ensemble *e, int parity, int mu, double angle, int reverse) {
     const SweepLayout &L = e->layouts[e->sweep_layout];
     const dim3 grid((unsigned)L.ctas), block(T);
     const Tile *items = L.d_items;
     switch (mu) {
-    case 0: k_su3_metropolis_ring<0, K><<<grid, block, kRingBytes, e->stream>>>(e->d_chains, items, e->d_links, parity, angle, e->d_sweep, e->d_accepts, L.log2_item); break;
-    case 1: k_su3_metropolis_ring<1, K><<<grid, block, kRingBytes, e->stream>>>(e->d_chains, items, e->d_links, parity, angle, e->d_sweep, e->d_accepts, L.log2_item); break;
-    case 2: k_su3_metropolis_ring<2, K><<<grid, block, kRingBytes, e->stream>>>(e->d_chains, items, e->d_links, parity, angle, e->d_sweep, e->d_accepts, L.log2_item); break;
-    default: k_su3_metropolis_ring<3, K><<<grid, block, kRingBytes, e->stream>>>(e->d_chains, items, e->d_links, parity, angle, e->d_sweep, e->d_accepts, L.log2_item); break;
+    case 0: k_su3_metropolis_ring<0, K><<<grid, block, kRingBytes, e->stream>>>(e->d_chains, items, e->d_links, parity, angle, e->d_sweep, e->d_accepts, L.log2_item, reverse); break;
+    case 1: k_su3_metropolis_ring<1, K><<<grid, block, kRingBytes, e->stream>>>(e->d_chains, items, e->d_links, parity, angle, e->d_sweep, e->d_accepts, L.log2_item, reverse); break;
+    case 2: k_su3_metropolis_ring<2, K><<<grid, block, kRingBytes, e->stream>>>(e->d_chains, items, e->d_links, parity, angle, e->d_sweep, e->d_accepts, L.log2_item, reverse); break;
+    default: k_su3_metropolis_ring<3, K><<<grid, block, kRingBytes, e->stream>>>(e->d_chains, items, e->d_links, parity, angle, e->d_sweep, e->d_accepts, L.log2_item, reverse); break;
     }
 }
 
-void metro_launch_drawn(ym_ensemble *e, int parity, int mu, double angle) {
+void metro_launch_drawn(ym_ensemble *e, int parity, int mu, double angle, int reverse) {
     const SweepLayout &L = e->layouts[e->sweep_layout];
     const dim3 grid((unsigned)L.ctas), block(T);
     const Tile *items = L.d_items;
     switch (mu) {
-    case 0: k_su3_metropolis<0><<<grid, block, kStageBytes, e->stream>>>(e->d_chains, items, e->d_links, parity, angle, 1, e->d_sweep, e->d_accepts, L.log2_item); break;
-    case 1: k_su3_metropolis<1><<<grid, block, kStageBytes, e->stream>>>(e->d_chains, items, e->d_links, parity, angle, 1, e->d_sweep, e->d_accepts, L.log2_item); break;
-    case 2: k_su3_metropolis<2><<<grid, block, kStageBytes, e->stream>>>(e->d_chains, items, e->d_links, parity, angle, 1, e->d_sweep, e->d_accepts, L.log2_item); break;
-    default: k_su3_metropolis<3><<<grid, block, kStageBytes, e->stream>>>(e->d_chains, items, e->d_links, parity, angle, 1, e->d_sweep, e->d_accepts, L.log2_item); break;
+    case 0: k_su3_metropolis<0><<<grid, block, kStageBytes, e->stream>>>(e->d_chains, items, e->d_links, parity, angle, 1, e->d_sweep, e->d_accepts, L.log2_item, reverse); break;
+    case 1: k_su3_metropolis<1><<<grid, block, kStageBytes, e->stream>>>(e->d_chains, items, e->d_links, parity, angle, 1, e->d_sweep, e->d_accepts, L.log2_item, reverse); break;
+    case 2: k_su3_metropolis<2><<<grid, block, kStageBytes, e->stream>>>(e->d_chains, items, e->d_links, parity, angle, 1, e->d_sweep, e->d_accepts, L.log2_item, reverse); break;
+    default: k_su3_metropolis<3><<<grid, block, kStageBytes, e->stream>>>(e->d_chains, items, e->d_links, parity, angle, 1, e->d_sweep, e->d_accepts, L.log2_item, reverse); break;
     }
 }
 
@@ -852,9 +854,14 @@ cudaError_t tiled_launch(ym_ensemble *e, int parity, int mu, double angle, int u
             if (cudaError_t err = set_smem(f, kRingBytes)) return err;
         configured_device = dev;
     }
-    if (uniform) metro_launch_drawn(e, parity, mu, angle);
-    else if (angle <= 0.3) metro_launch_ordered<11>(e, parity, mu, angle);
-    else metro_launch_ordered<14>(e, parity, mu, angle);
+    // Consecutive sub-sweeps walk the lattice in opposite directions (odd
+    // ones from the last CTA down), so each starts on the links the previous
+    // one touched last and finds its first waves' staple links in L2.  The
+    // links of one sub-sweep are independent, so the order changes no bit.
+    const int reverse = (parity * 4 + mu) & 1;
+    if (uniform) metro_launch_drawn(e, parity, mu, angle, reverse);
+    else if (angle <= 0.3) metro_launch_ordered<11>(e, parity, mu, angle, reverse);
+    else metro_launch_ordered<14>(e, parity, mu, angle, reverse);
     return cudaGetLastError();
 }
 
