@@ -95,7 +95,8 @@ __global__ void __launch_bounds__(kSiteThreads)
 k_f32_plaquette(const ChainInfo *__restrict__ chains, const Tile *__restrict__ tiles,
                 const float2 *__restrict__ links, double *__restrict__ partial) {
     __shared__ double warp_vals[32];
-    const Tile tile = tiles[blockIdx.x];
+    const int64_t tix = serpentine_tile(blockIdx.x, gridDim.x);   // tiles in serpentine order
+    const Tile tile = tiles[tix];
     const ChainInfo c = chains[tile.chain];
     const int64_t s = tile.start + threadIdx.x;
     double v = 0.0;
@@ -125,7 +126,7 @@ k_f32_plaquette(const ChainInfo *__restrict__ chains, const Tile *__restrict__ t
         v = threadIdx.x < (blockDim.x >> 5) ? warp_vals[threadIdx.x] : 0.0;
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-        if (threadIdx.x == 0) partial[blockIdx.x] = v;
+        if (threadIdx.x == 0) partial[tix] = v;
     }
 }
 

@@ -89,18 +89,20 @@ __device__ __forceinline__ double site_plaquette_sum_staged(const double2 *links
 }
 
 // Sum of the six plaquette values (1/3) Re Tr P of each site, site order
-// (mu, nu) = (0,1),(0,2),(0,3),(1,2),(1,3),(2,3), per tile.
+// (mu, nu) = (0,1),(0,2),(0,3),(1,2),(1,3),(2,3), per tile; tiles visited in
+// serpentine order.
 __global__ void __launch_bounds__(kSiteThreads)
 k_su3_plaquette(const ChainInfo *__restrict__ chains, const Tile *__restrict__ tiles,
                 const double2 *__restrict__ links, double *__restrict__ partial) {
-    const Tile tile = tiles[blockIdx.x];
+    const int64_t tix = serpentine_tile(blockIdx.x, gridDim.x);
+    const Tile tile = tiles[tix];
     const ChainInfo c = chains[tile.chain];
     const int64_t s = tile.start + threadIdx.x;
     extern __shared__ __align__(16) double2 plaq_stage_mem[];
     double v = 0.0;
     if (s < c.volume) v = site_plaquette_sum_staged(links, c, s, plaq_stage_mem);
     v = block_reduce<false>(v);
-    if (threadIdx.x == 0) partial[blockIdx.x] = v;
+    if (threadIdx.x == 0) partial[tix] = v;
 }
 
 // One block per chain: fixed-order reduction of the chain's tile partials.

@@ -251,6 +251,19 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
+// Tile visited by block b of n in serpentine order: the first half of the
+// tiles in order, the second half from the last tile down.  A site-tile
+// kernel launched right after a sweep whose last sub-sweep ended at the
+// lattice's start begins there (the links it touched last sit in L2), and
+// ends there again for the next sweep's first sub-sweep: with checkerboard
+// storage the first half of a chain's site tiles are its even sites, the
+// second half its odd ones, both in lexicographic order.  Results keyed by
+// tile are unchanged by the order.
+__device__ __forceinline__ int64_t serpentine_tile(int64_t b, int64_t n) {
+    const int64_t h = n / 2;
+    return b < h ? b : n - 1 - (b - h);
+}
+
 // ---------------------------------------------------------------- geometry
 
 // One chain of an ensemble.  Sites are stored in checkerboard order when the
