@@ -62,7 +62,10 @@ k_f32_metropolis(const ChainInfo *__restrict__ chains, const Tile *__restrict__ 
 __global__ void __launch_bounds__(kSiteThreads)
 k_f32_reunitarize(const ChainInfo *__restrict__ chains, const Tile *__restrict__ tiles,
                   float2 *__restrict__ links) {
-    const Tile tile = tiles[blockIdx.x];
+    // serpentine tile order: starts where the sweep's last sub-sweep ended
+    // and ends where the plaquette that follows starts (per-site work, so
+    // the order changes nothing else)
+    const Tile tile = tiles[serpentine_tile(blockIdx.x, gridDim.x)];
     const ChainInfo c = chains[tile.chain];
     const int64_t s = tile.start + threadIdx.x;
     if (s >= c.volume) return;
