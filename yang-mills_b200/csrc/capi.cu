@@ -1337,7 +1337,7 @@ int32_t ym_su3_spatial_stout_smear(ym_ensemble *src, ym_ensemble *dst, double rh
     }
     for (int64_t k = 1; k <= levels; ++k) {
         double2 *out = ((levels - k) % 2 == 0) ? dst->d_links : dst->d_links_tmp;
-        YM_CUDA(timed(dst, YM_KERNEL_STOUT, [&] { return ym::launch_stout_level(dst, in, out, rho); }));
+        YM_CUDA(timed(dst, YM_KERNEL_STOUT, [&] { return ym::launch_stout_level(dst, in, out, rho, (int)(k & 1)); }));
         in = out;
     }
     return take_device_error(dst);
@@ -1461,7 +1461,7 @@ static int32_t glueball_graph(ym_ensemble *ens, ym_ensemble *sm, const ym_glueba
         for (int32_t i = 0; i < plan->n_levels && err == cudaSuccess; ++i) {
             for (int64_t k = done; k < plan->levels[i] && err == cudaSuccess; ++k) {
                 double2 *out = cur == sm->d_links ? sm->d_links_tmp : sm->d_links;
-                err = ym::launch_stout_level(sm, cur, out, plan->rho);
+                err = ym::launch_stout_level(sm, cur, out, plan->rho, (int)((k + 1) & 1));   // the copy ends at the last tile
                 cur = out;
             }
             done = plan->levels[i] > done ? plan->levels[i] : done;

@@ -140,8 +140,8 @@ __device__ __forceinline__ m3 lk(const double2 *links, const ChainInfo &c, const
 __global__ void __launch_bounds__(T, 3)
 k_stout_level(const ChainInfo *__restrict__ chains, const Tile *__restrict__ tiles,
               const double2 *__restrict__ in, double2 *__restrict__ out, double rho,
-              unsigned *__restrict__ err) {
-    const Tile tile = tiles[blockIdx.x];
+              unsigned *__restrict__ err, int reverse) {
+    const Tile tile = tiles[reverse ? gridDim.x - 1 - blockIdx.x : blockIdx.x];
     const ChainInfo c = chains[tile.chain];
     const int64_t s = tile.start + threadIdx.x;
     if (s >= c.volume) return;
@@ -225,9 +225,9 @@ k_stout_level(const ChainInfo *__restrict__ chains, const Tile *__restrict__ til
 
 }  // namespace
 
-cudaError_t launch_stout_level(ym_ensemble *e, const double2 *in, double2 *out, double rho) {
+cudaError_t launch_stout_level(ym_ensemble *e, const double2 *in, double2 *out, double rho, int reverse) {
     k_stout_level<<<(unsigned)e->n_site_tiles, T, 0, e->stream>>>(e->d_chains, e->d_mixed_tiles, in, out,
-                                                                 rho, e->d_error);
+                                                                 rho, e->d_error, reverse);
     return cudaGetLastError();
 }
 

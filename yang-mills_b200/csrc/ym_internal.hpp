@@ -229,7 +229,10 @@ cudaError_t launch_polyakov(ym_ensemble *e, int dir, double *d_partial, double *
 cudaError_t launch_operator_basis(ym_ensemble *e, double2 *d_site_vals, const int32_t *d_slice_chain,
                                   const int32_t *d_slice_t, int64_t n_slices, double *d_plaq,
                                   double *d_rect, const double2 *links = nullptr);
-cudaError_t launch_stout_level(ym_ensemble *e, const double2 *in, double2 *out, double rho);
+// One stout level in -> out.  Consecutive levels pass reverse = 0, 1, 0, ...
+// so each walks its tiles opposite to the last and starts on the links the
+// previous level wrote last (in L2); per-site work, so no bit changes.
+cudaError_t launch_stout_level(ym_ensemble *e, const double2 *in, double2 *out, double rho, int reverse);
 cudaError_t launch_block(ym_ensemble *fine, ym_ensemble *coarse);
 // Per-chain means of tile partials [tile][width] (loops: / volume; dir >= 0:
 // / number of lines along dir), fixed order.
