@@ -276,34 +276,34 @@ def main():
     links = 4 * volume
     peak, peak_kind = measured_peaks()
 
-    def timed_leg(ens, step, link_bytes, kernel, sampler_clocks=False):
-        """W warm-up steps, then args.steps steps (step() = one sweep) each
-        followed by the plaquette, timed with CUDA events on the handle's
-        stream; per-launch time of the dominant kernel from event pairs.
-        With sampler_clocks, nvidia-smi samples every 10 ms from before the
-        warm-up to after the timed steps: "clocks" summarises the samples
-        inside the timed region, "clocks_leg" all of them."""
+    def timed_leg(ens, step, link_bytes, kernel, measured, sampler_clocks=False):
+        """The run_chain cadence of one leg: W warm-up steps, then args.steps
+        steps (one sweep, then the average plaquette of the swept lattice),
+        timed with CUDA events on the handle's stream.  measured(n) runs n
+        steps through the library's measured-sweeps entry point (one captured
+        graph per step, the plaquette of every step stored on the device and
+        read back once at the end) and returns the plaquette series.  A second
+        pass of the same steps issued one launch at a time with event pairs
+        around each launch (step() = one sweep, then average_plaquette) gives
+        the dominant kernel's per-launch time and its share of a step.  With
+        sampler_clocks, nvidia-smi samples every 10 ms from before the warm-up
+        to after the timed steps: "clocks" summarises the samples inside the
+        timed region, "clocks_leg" all of them."""
         sampler = ClockSampler(local) if sampler_clocks else None
         if sampler:
             sampler.__enter__()
             sampler.wait_first()
-        for _ in range(args.warmup):
-            step()
-            ens.average_plaquette()
+        measured(args.warmup)
         ens.synchronize()
         stream = torch.cuda.ExternalStream(ens.stream(), device=local)
         start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         p0, a0 = ens.accounting()
-        plaq = []
-        ens.profile(True)
         barrier()
         torch.cuda.synchronize()
         if sampler:
             sampler.wait_first()
         start.record(stream)
-        for _ in range(args.steps):
-            step()
-            plaq.append(float(ens.average_plaquette()[0]))
+        series = measured(args.steps)
         stop.record(stream)
         stop.synchronize()
         torch.cuda.synchronize()
@@ -312,9 +312,20 @@ def main():
             sampler.__exit__(None, None, None)
         barrier()
         ms = max_over_ranks(start.elapsed_time(stop))
+        p1, a1 = ens.accounting()
+        plaq = [float(v) for v in np.asarray(series)[:, 0]]
+        # per-launch pass
+        n_prof = max(3, min(args.steps, 20))
+        ens.profile(True)
+        pa, pb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        pa.record(stream)
+        for _ in range(n_prof):
+            step()
+            ens.average_plaquette()
+        pb.record(stream)
+        pb.synchronize()
         k_ms, k_launches = ens.profile_read(kernel)
         ens.profile(False)
-        p1, a1 = ens.accounting()
         launch_s = k_ms * 1e-3 / max(1, k_launches)
         bytes_per_launch = (volume // 2) * LINKS_PER_UPDATE * link_bytes
         achieved = bytes_per_launch / launch_s / 1e9
@@ -323,8 +334,10 @@ def main():
             "acceptance": float((a1 - a0)[0]) / float((p1 - p0)[0]),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
-                         "launch_ms": launch_s * 1e3, "kernel_share_of_step": k_ms / ms,
-                         "bytes_per_launch": bytes_per_launch},
+                         "launch_ms": launch_s * 1e3,
+                         "kernel_share_of_step": k_ms / max(1e-9, pa.elapsed_time(pb)),
+                         "bytes_per_launch": bytes_per_launch,
+                         "per_launch_pass_steps": n_prof},
             "clocks": sampler.summary() if sampler else None,
             "clocks_leg": sampler.summary(whole=True) if sampler else None,
         }
@@ -353,18 +366,20 @@ def main():
     p_gen, s_half = ymgpu.learned.proposal(model.forward(f_rec))
 
     # FP32 plain leg (ordered generators, half width 0.3)
-    f32 = timed_leg(t32, lambda: t32.metropolis_sweeps(ANGLE, 1), 48, "su3_metropolis")
+    f32 = timed_leg(t32, lambda: t32.metropolis_sweeps(ANGLE, 1), 48, "su3_metropolis",
+                    lambda n: t32.measured_sweeps(ANGLE, n, 1, "ordered"))
     # learned leg from the same starting lattice
     tl = t32.like()
     t32.copy_to(tl)
-    lrn = timed_leg(tl, lambda: model.sweeps(tl, 1), 48, "learned")
+    lrn = timed_leg(tl, lambda: model.sweeps(tl, 1), 48, "learned",
+                    lambda n: model.measured_sweeps(tl, n, 1))
     tl.close()
     # FP64 headline leg
     ens = t32.like(precision=ymgpu.F64)
     t32.convert_to(ens)
     t32.close()
     leg = timed_leg(ens, lambda: ens.metropolis_sweeps(ANGLE, 1), LINK_BYTES, "su3_metropolis",
-                    sampler_clocks=True)
+                    lambda n: ens.measured_sweeps(ANGLE, n, 1, "ordered"), sampler_clocks=True)
     ms, plaq = leg["ms"], leg["plaq"]
     roofline = dict(leg["roofline"])
     roofline.update({"traffic": ncu_traffic_per_launch(),
@@ -378,7 +393,8 @@ def main():
     ens.copy_to(fast_src)
     fast_src.sweep_index = ens.sweep_index
     fast_src.fast_sweeps = True
-    fleg = timed_leg(fast_src, lambda: fast_src.metropolis_sweeps(ANGLE, 1), LINK_BYTES, "su3_metropolis")
+    fleg = timed_leg(fast_src, lambda: fast_src.metropolis_sweeps(ANGLE, 1), LINK_BYTES, "su3_metropolis",
+                     lambda n: fast_src.measured_sweeps(ANGLE, n, 1, "ordered"))
     pair = []
     for fast in (False, True):
         c = fast_src.like()
@@ -739,11 +755,13 @@ def main():
                                    "wide-angle sweeps",
                        "lattice": "32^4", "global_batch": world, "parallelism": f"replicas x{world}",
                        "l2": "inputs 604 MB > 126 MB L2 (no flush)",
-                       "step": "1 checkerboard sweep + average plaquette"},
+                       "step": "1 checkerboard sweep + average plaquette (run_chain cadence through "
+                               "ym_su3_measured_sweeps: one captured graph per step, plaquettes kept in a "
+                               "device series and read back once)"},
             "plaquette_mean": float(np.mean(plaq)),
             "acceptance": leg["acceptance"],
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-            "gpu_launches": int(args.steps * 11),
+            "gpu_launches": int(args.steps * 12),   # 8 sub-sweeps, sweep counter, plaquette, reduction, series store
             "clocks": leg["clocks"],
             "clocks_leg": dict(leg["clocks_leg"] or {}, note="every sample of the FP64 leg: "
                                "warm-up, timed steps and the sampler's start and stop"),
