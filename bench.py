@@ -57,7 +57,7 @@ LOOP_EVERY = 10                       # sweeps between Wilson / Polyakov measure
 FAST_CHECK_SWEEPS = 10                # sweeps per form when the fast form is compared with the exact one
 MASTER_SEED = 0x2C02198105010002
 LINK_BYTES = 144                      # FP64 3x3 complex
-E2E_LATTICES = 3                      # independent lattices in flight end to end (upload, sweep, download)
+E2E_LATTICES = 4                      # independent lattices in flight end to end (upload, sweep, download)
 LINKS_PER_UPDATE = 9                  # 8 link reads + 1 write per checkerboard update
 FALLBACK_HBM_GBS = 6650.0
 
