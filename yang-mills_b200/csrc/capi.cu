@@ -158,6 +158,8 @@ void free_all(ym_ensemble *e) {
         if (p) ym::dev_free(p);
     for (auto &l : e->layouts)
         if (l.d_items) ym::dev_free(l.d_items);
+    for (auto &l : e->layouts)
+        if (l.d_chain_ctas) ym::dev_free(l.d_chain_ctas);
     if (e->stream) cudaStreamDestroy(e->stream);
 }
 
@@ -476,6 +478,22 @@ int32_t ym_ensemble_create(const ym_ensemble_desc *desc, ym_ensemble **out) {
             e->layouts[li].by_volume = li % 2;
         }
     }
+    // each chain's CTA range in the 128-site layouts (one chain per CTA, a
+    // chain's CTAs consecutive)
+    std::vector<std::vector<int32_t>> chain_ctas(ym::kSweepLayouts);
+    for (int li = 0; li < ym::kSweepLayouts; ++li) {
+        if (e->layouts[li].log2_item != 7) continue;
+        std::vector<int32_t> &r = chain_ctas[(size_t)li];
+        r.assign(2 * (size_t)e->n_chains, 0);
+        std::vector<bool> seen((size_t)e->n_chains, false);
+        for (size_t b = 0; b < lay[(size_t)li].size(); ++b) {
+            const int32_t ch = lay[(size_t)li][b].chain;
+            if (ch < 0) continue;
+            if (!seen[(size_t)ch]) r[2 * (size_t)ch] = (int32_t)b;
+            seen[(size_t)ch] = true;
+            r[2 * (size_t)ch + 1] = (int32_t)b + 1;
+        }
+    }
 
     cudaError_t err = cudaSetDevice(e->device);
     if (err == cudaSuccess) err = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
@@ -501,6 +519,13 @@ int32_t ym_ensemble_create(const ym_ensemble_desc *desc, ym_ensemble **out) {
     if (err == cudaSuccess && !half.empty())
         err = cudaMemcpy(e->d_half_tiles, half.data(), half.size() * sizeof(Tile), cudaMemcpyHostToDevice);
     for (int li = 0; li < ym::kSweepLayouts && err == cudaSuccess; ++li) {
+        if (!chain_ctas[(size_t)li].empty()) {
+            err = dalloc(&e->layouts[li].d_chain_ctas, chain_ctas[(size_t)li].size());
+            if (err == cudaSuccess)
+                err = cudaMemcpy(e->layouts[li].d_chain_ctas, chain_ctas[(size_t)li].data(),
+                                 chain_ctas[(size_t)li].size() * sizeof(int32_t), cudaMemcpyHostToDevice);
+            if (err != cudaSuccess) break;
+        }
         err = dalloc(&e->layouts[li].d_items, lay[(size_t)li].size());
         if (err == cudaSuccess && !lay[(size_t)li].empty())
             err = cudaMemcpy(e->layouts[li].d_items, lay[(size_t)li].data(), lay[(size_t)li].size() * sizeof(Tile),
@@ -756,6 +781,44 @@ static void drop_run_graph(ym_ensemble *e) {
     e->run_graph = nullptr;
 }
 
+// The run_chain cadence's plaquette after a sweep.  For binary64 handles
+// with ordered hits, one chain per sub-sweep CTA and chains too large for
+// the chain-resident kernel, the sweep's last sub-sweep (parity 1,
+// direction 3) also sums, per CTA, (1/3) Re Tr(U' A) of its links: every
+// link of those staples is final then, and each plaquette of planes (0,3),
+// (1,3), (2,3) holds exactly one odd-site 3-link, so the sums are those
+// planes' plaquettes; a three-plane kernel adds (0,1), (0,2), (1,2).  The
+// average plaquette then agrees with ym_average_plaquette's to rounding
+// (different summation order) for half the plaquette kernel's work.
+static bool fused_plaquette(const ym_ensemble *e, int mode) {
+    return e->group == YM_GROUP_SU3 && !f32(e) && mode == YM_GEN_ORDERED &&
+           e->layouts[e->sweep_layout].d_chain_ctas && !ym::resident_fits(e);
+}
+
+// One sweep of the cadence (measure: the last sub-sweep also writes its
+// plaquette shares to d_partial2).
+static cudaError_t cadence_sweep(ym_ensemble *e, double angle, int mode, bool measure) {
+    for (int parity = 0; parity < 2; ++parity)
+        for (int mu = 0; mu < 4; ++mu) {
+            cudaError_t err;
+            if (f32(e)) err = ym::launch_f32_metropolis(e, parity, mu, angle, mode);
+            else if (measure && parity == 1 && mu == 3) err = ym::launch_su3_metropolis_measure(e, angle, e->d_partial2);
+            else err = ym::launch_su3_metropolis(e, parity, mu, angle, mode);
+            if (err != cudaSuccess) return err;
+        }
+    cudaError_t err = f32(e) ? ym::launch_f32_reunitarize(e) : cudaSuccess;
+    return err == cudaSuccess ? ym::launch_advance_sweep(e) : err;
+}
+
+// The average plaquette of every chain into d_result after cadence_sweep.
+static cudaError_t cadence_plaquette(ym_ensemble *e, bool fused) {
+    if (f32(e)) {
+        cudaError_t err = ym::launch_f32_plaquette_partials(e);
+        return err == cudaSuccess ? ym::launch_chain_reduce(e, e->d_partial, e->d_result, 0, 6.0) : err;
+    }
+    return fused ? ym::launch_su3_plaquette_split(e, e->d_partial2) : ym::launch_su3_plaquette(e);
+}
+
 static cudaError_t ensure_series(ym_ensemble *e, int64_t n_measurements) {
     if (e->series_capacity < n_measurements) {
         if (e->measure_graph) cudaGraphExecDestroy(e->measure_graph);
@@ -794,20 +857,13 @@ int32_t ym_su3_measured_sweeps(ym_ensemble *e, double angle, int32_t generator_m
     if (n_measurements == 0) return YM_OK;
     YM_CUDA(ensure_series(e, n_measurements));
     YM_CUDA(cudaMemsetAsync(e->d_series_row, 0, sizeof(uint64_t), e->stream));
+    const bool fused = sweeps_per_measurement > 0 && fused_plaquette(e, generator_mode);
     auto step = [&]() -> cudaError_t {
         for (int64_t k = 0; k < sweeps_per_measurement; ++k) {
-            for (int parity = 0; parity < 2; ++parity)
-                for (int mu = 0; mu < 4; ++mu) {
-                    cudaError_t err = f32(e) ? ym::launch_f32_metropolis(e, parity, mu, angle, generator_mode)
-                                             : ym::launch_su3_metropolis(e, parity, mu, angle, generator_mode);
-                    if (err != cudaSuccess) return err;
-                }
-            cudaError_t err = f32(e) ? ym::launch_f32_reunitarize(e) : cudaSuccess;
-            if (err == cudaSuccess) err = ym::launch_advance_sweep(e);
+            cudaError_t err = cadence_sweep(e, angle, generator_mode, fused && k == sweeps_per_measurement - 1);
             if (err != cudaSuccess) return err;
         }
-        cudaError_t err = f32(e) ? ym::launch_f32_plaquette_partials(e) : ym::launch_su3_plaquette(e);
-        if (err == cudaSuccess && f32(e)) err = ym::launch_chain_reduce(e, e->d_partial, e->d_result, 0, 6.0);
+        cudaError_t err = cadence_plaquette(e, fused);
         if (err == cudaSuccess) err = ym::launch_store_series(e, e->d_series, e->d_series_row);
         return err;
     };
@@ -919,18 +975,11 @@ int32_t ym_su3_measured_run(ym_ensemble *e, ym_ensemble *view, const ym_measured
     YM_CUDA(cudaMemsetAsync(e->d_series_row, 0, sizeof(uint64_t), e->stream));
     YM_CUDA(cudaMemsetAsync(e->d_loop_row, 0, sizeof(uint64_t), e->stream));
     const double angle = run->proposal_angle;
+    const bool fused = fused_plaquette(e, mode);
     auto block = [&]() -> cudaError_t {
         for (int64_t k = 0; k < spb; ++k) {
-            for (int parity = 0; parity < 2; ++parity)
-                for (int mu = 0; mu < 4; ++mu) {
-                    cudaError_t err = f32(e) ? ym::launch_f32_metropolis(e, parity, mu, angle, mode)
-                                             : ym::launch_su3_metropolis(e, parity, mu, angle, mode);
-                    if (err != cudaSuccess) return err;
-                }
-            cudaError_t err = f32(e) ? ym::launch_f32_reunitarize(e) : cudaSuccess;
-            if (err == cudaSuccess) err = ym::launch_advance_sweep(e);
-            if (err == cudaSuccess) err = f32(e) ? ym::launch_f32_plaquette_partials(e) : ym::launch_su3_plaquette(e);
-            if (err == cudaSuccess && f32(e)) err = ym::launch_chain_reduce(e, e->d_partial, e->d_result, 0, 6.0);
+            cudaError_t err = cadence_sweep(e, angle, mode, fused);
+            if (err == cudaSuccess) err = cadence_plaquette(e, fused);
             if (err == cudaSuccess) err = ym::launch_store_series(e, e->d_series, e->d_series_row);
             if (err != cudaSuccess) return err;
         }

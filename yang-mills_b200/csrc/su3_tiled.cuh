@@ -595,9 +595,10 @@ __device__ __forceinline__ void hit_diag_sel(m3 &u, const double2 (*sa)[T], doub
 
 // The eight ordered hits (generators 1..8, su3_ensemble.rs:361): hit h+1's
 // link-independent half is written next to hit h.
+// tr receives Re Tr(U' A) of the final link, the sum of its six plaquettes.
 template <int K>
 __device__ __forceinline__ unsigned visit_ordered(m3 &u, const double2 (*sa)[T], double beta3,
-                                                  double angle, uint64_t key) {
+                                                  double angle, uint64_t key, double &tr) {
     double rr[3];
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
@@ -623,6 +624,7 @@ __device__ __forceinline__ unsigned visit_ordered(m3 &u, const double2 (*sa)[T],
     const DiagPre p7 = pre_diag<K>(key, 7, angle);
     hit_block_sel<1, 2, 1>(u, sa, rr, old_tr, p6, beta3, accepted);
     hit_diag_sel(u, sa, rr, old_tr, p7, beta3, accepted);
+    tr = old_tr;
     return accepted;
 }
 
@@ -758,12 +760,17 @@ __device__ __forceinline__ m3 staple_ring(const double2 *links, const ChainInfo 
 
 constexpr int kRingBuffers = 6;   // two sets of three factors
 
-template <int MU, int K>
+// MEASURE (the last sub-sweep of a sweep, parity 1 and direction 3, with one
+// chain per CTA): each CTA also writes tr_partial[cta] = sum over its links
+// of (1/3) Re Tr(U' A).  Every link in the staple of an odd-site 3-link is
+// final by then, so this is the CTA's share of the plaquettes in planes
+// (0,3), (1,3), (2,3): each such plaquette holds exactly one odd-site 3-link.
+template <int MU, int K, bool MEASURE = false>
 __global__ void __launch_bounds__(T, 2)
 k_su3_metropolis_ring(const ChainInfo *__restrict__ chains, const Tile *__restrict__ tiles,
                       double2 *__restrict__ links, int parity, double angle,
                       const uint64_t *__restrict__ sweep_ptr, unsigned long long *__restrict__ accepts,
-                      int log2_item, int reverse) {
+                      int log2_item, int reverse, double *__restrict__ tr_partial = nullptr) {
     extern __shared__ __align__(16) double2 ring_mem[];
     auto buf = [&](int i) { return reinterpret_cast<double2 (*)[T]>(ring_mem + (size_t)i * 9 * T); };
     const TermSet s0{{buf(0), buf(1), buf(2)}}, s1{{buf(3), buf(4), buf(5)}};
@@ -774,6 +781,7 @@ k_su3_metropolis_ring(const ChainInfo *__restrict__ chains, const Tile *__restri
     const int64_t t = tile.start + (threadIdx.x & ((1u << log2_item) - 1u));
     const uint64_t sweep = *sweep_ptr;
     unsigned accepted = 0;
+    double tr = 0.0;
     if (live && t < c.half) {
         const int64_t s = (int64_t)parity * c.half + t;
         const Coord x = decode_storage(c, s);
@@ -786,12 +794,17 @@ k_su3_metropolis_ring(const ChainInfo *__restrict__ chains, const Tile *__restri
 #pragma unroll
         for (int e = 0; e < 9; ++e) sa[e][threadIdx.x] = make_double2(a.e[e / 3][e % 3].re, a.e[e / 3][e % 3].im);
         const uint64_t key = link_key(c.seed, sweep, x.lex, MU);
-        accepted = visit_ordered<K>(u, sa, c.beta / 3.0, angle, key);
+        accepted = visit_ordered<K>(u, sa, c.beta / 3.0, angle, key, tr);
         store_su3(links, c, s, MU, u);
     }
     const unsigned warp_sum = __reduce_add_sync(0xffffffffu, accepted);
     if ((threadIdx.x & 31) == 0 && warp_sum)
         atomicAdd(accepts + tile.chain, (unsigned long long)warp_sum);
+    if (MEASURE) {
+        double v = (live && t < c.half) ? tr / 3.0 : 0.0;
+        v = block_reduce<false>(v);
+        if (threadIdx.x == 0) tr_partial[cta] = v;
+    }
 }
 
 
@@ -827,6 +840,17 @@ void metro_launch_drawn(ym_ensemble *e, int parity, int mu, double angle, int re
     }
 }
 
+// The last sub-sweep of a sweep (parity 1, direction 3, ordered hits) with
+// its plaquette share (MEASURE): the handle's layout must put one chain in
+// each CTA (128-site items).
+template <int K>
+void metro_launch_measure(ym_ensemble *e, double angle, double *tr_partial) {
+    const SweepLayout &L = e->layouts[e->sweep_layout];
+    k_su3_metropolis_ring<3, K, true><<<(unsigned)L.ctas, T, kRingBytes, e->stream>>>(
+        e->d_chains, L.d_items, e->d_links, 1, angle, e->d_sweep, e->d_accepts, L.log2_item,
+        (1 * 4 + 3) & 1, tr_partial);
+}
+
 cudaError_t set_smem(const void *f, size_t bytes) {
     cudaError_t err = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     if (err == cudaSuccess)
@@ -834,26 +858,35 @@ cudaError_t set_smem(const void *f, size_t bytes) {
     return err;
 }
 
+// Shared-memory limits of the sub-sweep kernels, set once per device.
+cudaError_t configure_kernels() {
+    static thread_local int configured_device = -1;
+    int dev = 0;
+    cudaError_t err = cudaGetDevice(&dev);
+    if (err != cudaSuccess) return err;
+    if (configured_device != dev) {
+        const void *drawn[4] = {(const void *)k_su3_metropolis<0>, (const void *)k_su3_metropolis<1>,
+                                (const void *)k_su3_metropolis<2>, (const void *)k_su3_metropolis<3>};
+        const void *ordered[10] = {(const void *)k_su3_metropolis_ring<0, 11>, (const void *)k_su3_metropolis_ring<1, 11>,
+                                   (const void *)k_su3_metropolis_ring<2, 11>, (const void *)k_su3_metropolis_ring<3, 11>,
+                                   (const void *)k_su3_metropolis_ring<0, 14>, (const void *)k_su3_metropolis_ring<1, 14>,
+                                   (const void *)k_su3_metropolis_ring<2, 14>, (const void *)k_su3_metropolis_ring<3, 14>,
+                                   (const void *)k_su3_metropolis_ring<3, 11, true>,
+                                   (const void *)k_su3_metropolis_ring<3, 14, true>};
+        for (const void *f : drawn)
+            if ((err = set_smem(f, kStageBytes)) != cudaSuccess) return err;
+        for (const void *f : ordered)
+            if ((err = set_smem(f, kRingBytes)) != cudaSuccess) return err;
+        configured_device = dev;
+    }
+    return cudaSuccess;
+}
+
 // One sub-sweep of the handle: ordered hits on the ring kernel with the
 // term count the half width allows (angles are validated to lie in
 // [1e-8, 1] for binary64 handles), drawn generators on the three-CTA kernel.
 cudaError_t tiled_launch(ym_ensemble *e, int parity, int mu, double angle, int uniform) {
-    static thread_local int configured_device = -1;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (configured_device != dev) {
-        const void *drawn[4] = {(const void *)k_su3_metropolis<0>, (const void *)k_su3_metropolis<1>,
-                                (const void *)k_su3_metropolis<2>, (const void *)k_su3_metropolis<3>};
-        const void *ordered[8] = {(const void *)k_su3_metropolis_ring<0, 11>, (const void *)k_su3_metropolis_ring<1, 11>,
-                                  (const void *)k_su3_metropolis_ring<2, 11>, (const void *)k_su3_metropolis_ring<3, 11>,
-                                  (const void *)k_su3_metropolis_ring<0, 14>, (const void *)k_su3_metropolis_ring<1, 14>,
-                                  (const void *)k_su3_metropolis_ring<2, 14>, (const void *)k_su3_metropolis_ring<3, 14>};
-        for (const void *f : drawn)
-            if (cudaError_t err = set_smem(f, kStageBytes)) return err;
-        for (const void *f : ordered)
-            if (cudaError_t err = set_smem(f, kRingBytes)) return err;
-        configured_device = dev;
-    }
+    if (cudaError_t err = configure_kernels()) return err;
     // Consecutive sub-sweeps walk the lattice in opposite directions (odd
     // ones from the last CTA down), so each starts on the links the previous
     // one touched last and finds its first waves' staple links in L2.  The
@@ -862,6 +895,16 @@ cudaError_t tiled_launch(ym_ensemble *e, int parity, int mu, double angle, int u
     if (uniform) metro_launch_drawn(e, parity, mu, angle, reverse);
     else if (angle <= 0.3) metro_launch_ordered<11>(e, parity, mu, angle, reverse);
     else metro_launch_ordered<14>(e, parity, mu, angle, reverse);
+    return cudaGetLastError();
+}
+
+// tiled_launch(e, 1, 3, angle, ordered hits) that also writes each CTA's
+// plaquette share of planes (0,3), (1,3), (2,3) to tr_partial[cta] (the
+// handle's layout must hold one chain per CTA).
+cudaError_t tiled_launch_measure(ym_ensemble *e, double angle, double *tr_partial) {
+    if (cudaError_t err = configure_kernels()) return err;
+    if (angle <= 0.3) metro_launch_measure<11>(e, angle, tr_partial);
+    else metro_launch_measure<14>(e, angle, tr_partial);
     return cudaGetLastError();
 }
 

@@ -31,6 +31,9 @@ struct SweepLayout {
     int64_t ctas = 0;
     int32_t log2_item = 7;
     int32_t by_volume = 0;     // items of the largest chains first
+    // 128-site items (one chain per CTA): [2 * chain] first CTA, [2 * chain + 1]
+    // one past the last CTA of each chain; null for the other item sizes
+    int32_t *d_chain_ctas = nullptr;
 };
 constexpr int kSweepLayouts = 6;   // item sizes 128, 64, 32 x (chain order, by volume)
 
@@ -202,6 +205,15 @@ cudaError_t launch_su3_metropolis(ym_ensemble *e, int parity, int mu, double ang
 // The same sub-sweep in the fast form (su3_metropolis_fast.cu);
 // launch_su3_metropolis dispatches to it when e->fast_sweeps is set.
 cudaError_t launch_su3_metropolis_fast(ym_ensemble *e, int parity, int mu, double angle, int uniform);
+// The last sub-sweep of a sweep (parity 1, direction 3, ordered hits), also
+// writing each CTA's share of the plaquettes in planes (0,3), (1,3), (2,3)
+// to tr_partial[cta]; the handle's layout must hold one chain per CTA.
+cudaError_t launch_su3_metropolis_measure(ym_ensemble *e, double angle, double *tr_partial);
+cudaError_t launch_su3_metropolis_measure_fast(ym_ensemble *e, double angle, double *tr_partial);
+// After such a sweep: the plaquettes of planes (0,1), (0,2), (1,2) per site
+// tile, and each chain's average plaquette from both sets of partials
+// (tr_partial and the layout's per-chain CTA ranges) into d_result.
+cudaError_t launch_su3_plaquette_split(ym_ensemble *e, const double *tr_partial);
 cudaError_t launch_advance_sweep(ym_ensemble *e);
 // Chain-resident sweeps (su3_metropolis.cu): every chain small enough that
 // its links fit in one CTA's shared memory.  series (device, may be null)
