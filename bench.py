@@ -695,14 +695,14 @@ def main():
         h.sweep_index = ens.sweep_index + 1000 * i
     hosts = []
     for h in lattices:
+        h.measured_sweeps(ANGLE, 1, 1, "ordered")   # builds the handle's step graph before timing
         buf = torch.empty(links * 18, dtype=torch.float64, pin_memory=True)
         hosts.append(buf.numpy().view(np.complex128).reshape(links, 3, 3))
         h.download(0, hosts[-1])
 
     def e2e_step(h, host_np):
         h.upload(0, host_np)
-        h.metropolis_sweeps(ANGLE, 1)
-        h.average_plaquette()
+        h.measured_sweeps(ANGLE, 1, 1, "ordered")   # one sweep, its plaquette read back
         h.download(0, host_np)
 
     def e2e_worker(i, n, gate):
@@ -732,7 +732,7 @@ def main():
            "h2d_bytes_per_step": links * LINK_BYTES,
            "d2h_bytes_per_step": links * LINK_BYTES + 8,
            "steps": e2e_steps,
-           "path": "ym_ensemble_upload -> ym_su3_metropolis_sweeps -> ym_average_plaquette "
+           "path": "ym_ensemble_upload -> ym_su3_measured_sweeps (one sweep and its plaquette) "
                    f"-> ym_ensemble_download (pinned host lattice in the reference layout), {E2E_LATTICES} "
                    f"independent lattices on {E2E_LATTICES} host threads taking turns",
            "one_lattice": {"value": world * links * (e2e_steps // E2E_LATTICES) / e2e_one_s, "unit": UNIT,
