@@ -121,9 +121,10 @@ k_su3_plaquette3(const ChainInfo *__restrict__ chains, const Tile *__restrict__ 
     if (threadIdx.x == 0) partial[tix] = v;
 }
 
-// One block per chain: its site-tile partials (planes (0,1), (0,2), (1,2))
-// and its sub-sweep CTA partials (planes (0,3), (1,3), (2,3)), each summed
-// in a fixed order, then the average plaquette sum / (6 V).
+// One 1024-thread block per chain: its site-tile partials (planes (0,1),
+// (0,2), (1,2)) and its sub-sweep CTA partials (planes (0,3), (1,3),
+// (2,3)), each summed in a fixed order, then the average plaquette
+// sum / (6 V).
 __global__ void k_chain_reduce_split(const double *__restrict__ site_partial, const int32_t *__restrict__ first,
                                      const double *__restrict__ cta_partial, const int32_t *__restrict__ cta_range,
                                      const ChainInfo *__restrict__ chains, double *__restrict__ out) {
@@ -502,7 +503,7 @@ cudaError_t launch_su3_plaquette_split(ym_ensemble *e, const double *tr_partial)
     if (!ranges) return cudaErrorInvalidValue;
     k_su3_plaquette3<<<(unsigned)e->n_site_tiles, kSiteThreads, kPlaqStageBytes, e->stream>>>(
         e->d_chains, e->d_site_tiles, e->d_links, e->d_partial);
-    k_chain_reduce_split<<<(unsigned)e->n_chains, 256, 0, e->stream>>>(
+    k_chain_reduce_split<<<(unsigned)e->n_chains, 1024, 0, e->stream>>>(
         e->d_partial, e->d_site_tile_first, tr_partial, ranges, e->d_chains, e->d_result);
     return cudaGetLastError();
 }
