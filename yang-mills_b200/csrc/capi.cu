@@ -153,7 +153,8 @@ void free_all(ym_ensemble *e) {
                     e->d_result2, e->d_accepts, e->d_sweep, e->d_rng, e->d_ref_counts,
                     e->d_error, e->d_obs_partial, e->d_obs_out, e->d_site_vals,
                     e->d_slice_chain, e->d_slice_t, e->d_slice_plaq, e->d_slice_rect,
-                    e->d_links_tmp, e->d_query_error, e->d_query, e->d_steps, e->d_terms};
+                    e->d_links_tmp, e->d_query_error, e->d_query, e->d_steps, e->d_terms,
+                    e->d_tr_partial};
     for (void *p : ptrs)
         if (p) ym::dev_free(p);
     for (auto &l : e->layouts)
@@ -514,6 +515,10 @@ int32_t ym_ensemble_create(const ym_ensemble_desc *desc, ym_ensemble **out) {
     if (err == cudaSuccess) err = dalloc(&e->d_ref_counts, 2 * (size_t)e->n_chains);
     if (err == cudaSuccess) err = dalloc(&e->d_error, 1);
     if (err == cudaSuccess) err = cudaMemset(e->d_error, 0, sizeof(unsigned));
+    // plaquette shares of a measured sweep: three arrays of the 128-site
+    // layouts' CTA count (binary64 SU(3))
+    if (err == cudaSuccess && e->group == YM_GROUP_SU3 && e->precision == YM_PREC_F64)
+        err = dalloc(&e->d_tr_partial, 3 * (size_t)e->layouts[0].ctas);
     if (err == cudaSuccess)
         err = cudaMemcpy(e->d_chains, e->chains.data(), e->chains.size() * sizeof(ChainInfo), cudaMemcpyHostToDevice);
     if (err == cudaSuccess && !half.empty())
@@ -783,26 +788,28 @@ static void drop_run_graph(ym_ensemble *e) {
 
 // The run_chain cadence's plaquette after a sweep.  For binary64 handles
 // with ordered hits, one chain per sub-sweep CTA and chains too large for
-// the chain-resident kernel, the sweep's last sub-sweep (parity 1,
-// direction 3) also sums, per CTA, (1/3) Re Tr(U' A) of its links: every
-// link of those staples is final then, and each plaquette of planes (0,3),
-// (1,3), (2,3) holds exactly one odd-site 3-link, so the sums are those
-// planes' plaquettes; a three-plane kernel adds (0,1), (0,2), (1,2).  The
-// average plaquette then agrees with ym_average_plaquette's to rounding
-// (different summation order) for half the plaquette kernel's work.
+// the chain-resident kernel, the sweep's last three sub-sweeps (parity 1,
+// directions 1, 2, 3) also sum, per CTA, (1/3) Re Tr(U' A_p) of their links,
+// A_p the staple terms of the lower directions: all those links are final
+// then, and each plaquette of plane (nu, mu) holds exactly one odd-site
+// mu-link, so the three sums are the six planes' plaquettes and no
+// plaquette kernel runs.  The average plaquette agrees with
+// ym_average_plaquette's to rounding (different summation order).
 static bool fused_plaquette(const ym_ensemble *e, int mode) {
-    return e->group == YM_GROUP_SU3 && !f32(e) && mode == YM_GEN_ORDERED &&
+    return e->group == YM_GROUP_SU3 && !f32(e) && mode == YM_GEN_ORDERED && e->d_tr_partial &&
            e->layouts[e->sweep_layout].d_chain_ctas && !ym::resident_fits(e);
 }
 
-// One sweep of the cadence (measure: the last sub-sweep also writes its
-// plaquette shares to d_partial2).
+// One sweep of the cadence (measure: sub-sweeps (1, mu), mu = 1..3, also
+// write their plaquette shares to d_tr_partial, one array of CTAs each).
 static cudaError_t cadence_sweep(ym_ensemble *e, double angle, int mode, bool measure) {
+    const int64_t ctas = e->layouts[e->sweep_layout].ctas;
     for (int parity = 0; parity < 2; ++parity)
         for (int mu = 0; mu < 4; ++mu) {
             cudaError_t err;
             if (f32(e)) err = ym::launch_f32_metropolis(e, parity, mu, angle, mode);
-            else if (measure && parity == 1 && mu == 3) err = ym::launch_su3_metropolis_measure(e, angle, e->d_partial2);
+            else if (measure && parity == 1 && mu >= 1)
+                err = ym::launch_su3_metropolis_measure(e, mu, angle, e->d_tr_partial + (mu - 1) * ctas);
             else err = ym::launch_su3_metropolis(e, parity, mu, angle, mode);
             if (err != cudaSuccess) return err;
         }
@@ -816,7 +823,7 @@ static cudaError_t cadence_plaquette(ym_ensemble *e, bool fused) {
         cudaError_t err = ym::launch_f32_plaquette_partials(e);
         return err == cudaSuccess ? ym::launch_chain_reduce(e, e->d_partial, e->d_result, 0, 6.0) : err;
     }
-    return fused ? ym::launch_su3_plaquette_split(e, e->d_partial2) : ym::launch_su3_plaquette(e);
+    return fused ? ym::launch_su3_plaquette_from_sweep(e, e->d_tr_partial) : ym::launch_su3_plaquette(e);
 }
 
 static cudaError_t ensure_series(ym_ensemble *e, int64_t n_measurements) {

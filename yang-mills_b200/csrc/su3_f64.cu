@@ -88,63 +88,22 @@ __device__ __forceinline__ double site_plaquette_sum_staged(const double2 *links
     return v;
 }
 
-// The three plaquettes of a site without direction 3, planes (0,1), (0,2),
-// (1,2), staged as in site_plaquette_sum_staged.
-__device__ __forceinline__ double site_plaquette_sum3_staged(const double2 *links, const ChainInfo &c, int64_t s,
-                                                             double2 *stage) {
-    const PlaqBuf b0 = reinterpret_cast<PlaqBuf>(stage);
-    const PlaqBuf c0 = reinterpret_cast<PlaqBuf>(stage + 9 * kSiteThreads);
-    const PlaqBuf b1 = reinterpret_cast<PlaqBuf>(stage + 18 * kSiteThreads);
-    const PlaqBuf c1 = reinterpret_cast<PlaqBuf>(stage + 27 * kSiteThreads);
-    const Coord x = decode_storage(c, s);
-    plaq_stage<0, 1>(b0, c0, links, c, x);
-    plaq_stage<0, 2>(b1, c1, links, c, x);
-    double v = plaq_plane<0, 1, true, 1, 2>(b0, c0, links, c, x, s);   // then (1,2) into set 0
-    v = v + plaq_plane<0, 2, false, 0, 0>(b1, c1, links, c, x, s);
-    v = v + plaq_plane<1, 2, false, 0, 0>(b0, c0, links, c, x, s);
-    return v;
-}
-
-// Per site tile (serpentine order), the plaquettes of planes (0,1), (0,2),
-// (1,2): the other three planes come from the sweep's last sub-sweep.
-__global__ void __launch_bounds__(kSiteThreads)
-k_su3_plaquette3(const ChainInfo *__restrict__ chains, const Tile *__restrict__ tiles,
-                 const double2 *__restrict__ links, double *__restrict__ partial) {
-    const int64_t tix = serpentine_tile(blockIdx.x, gridDim.x);
-    const Tile tile = tiles[tix];
-    const ChainInfo c = chains[tile.chain];
-    const int64_t s = tile.start + threadIdx.x;
-    extern __shared__ __align__(16) double2 plaq_stage_mem[];
-    double v = 0.0;
-    if (s < c.volume) v = site_plaquette_sum3_staged(links, c, s, plaq_stage_mem);
-    v = block_reduce<false>(v);
-    if (threadIdx.x == 0) partial[tix] = v;
-}
-
-// One 1024-thread block per chain: its site-tile partials (planes (0,1),
-// (0,2), (1,2)) and its sub-sweep CTA partials (planes (0,3), (1,3),
-// (2,3)), each summed in a fixed order, then the average plaquette
-// sum / (6 V).
-__global__ void k_chain_reduce_split(const double *__restrict__ site_partial, const int32_t *__restrict__ first,
-                                     const double *__restrict__ cta_partial, const int32_t *__restrict__ cta_range,
-                                     const ChainInfo *__restrict__ chains, double *__restrict__ out) {
+// One 1024-thread block per chain: the plaquette shares the last three
+// sub-sweeps of a sweep wrote for the chain's CTAs (planes (0,1); (0,2),
+// (1,2); (0,3), (1,3), (2,3)), summed CTA by CTA in a fixed order, then the
+// average plaquette sum / (6 V).
+__global__ void k_chain_reduce_sweep(const double *__restrict__ tr_partial, int64_t ctas,
+                                     const int32_t *__restrict__ cta_range, const ChainInfo *__restrict__ chains,
+                                     double *__restrict__ out) {
     const int chain = blockIdx.x;
+    const int b = cta_range[2 * chain], e = cta_range[2 * chain + 1];
     double v = 0.0;
-    {
-        const int b = first[chain], e = first[chain + 1];
-        for (int i = b + threadIdx.x; i < e; i += blockDim.x) v = (i == b + (int)threadIdx.x) ? site_partial[i] : v + site_partial[i];
+    for (int i = b + threadIdx.x; i < e; i += blockDim.x) {
+        const double p = (tr_partial[i] + tr_partial[ctas + i]) + tr_partial[2 * ctas + i];
+        v = (i == b + (int)threadIdx.x) ? p : v + p;
     }
     v = block_reduce<false>(v);
-    __shared__ double site_sum;
-    if (threadIdx.x == 0) site_sum = v;
-    __syncthreads();
-    double w = 0.0;
-    {
-        const int b = cta_range[2 * chain], e = cta_range[2 * chain + 1];
-        for (int i = b + threadIdx.x; i < e; i += blockDim.x) w = (i == b + (int)threadIdx.x) ? cta_partial[i] : w + cta_partial[i];
-    }
-    w = block_reduce<false>(w);
-    if (threadIdx.x == 0) out[chain] = (site_sum + w) / (6.0 * (double)chains[chain].volume);
+    if (threadIdx.x == 0) out[chain] = v / (6.0 * (double)chains[chain].volume);
 }
 
 // Sum of the six plaquette values (1/3) Re Tr P of each site, site order
@@ -489,22 +448,11 @@ cudaError_t launch_su3_plaquette(ym_ensemble *e) {
     return cudaGetLastError();
 }
 
-cudaError_t launch_su3_plaquette_split(ym_ensemble *e, const double *tr_partial) {
-    static thread_local int configured_device = -1;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (configured_device != dev) {
-        cudaError_t err = cudaFuncSetAttribute(k_su3_plaquette3, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               (int)kPlaqStageBytes);
-        if (err != cudaSuccess) return err;
-        configured_device = dev;
-    }
-    const int32_t *ranges = e->layouts[e->sweep_layout].d_chain_ctas;
-    if (!ranges) return cudaErrorInvalidValue;
-    k_su3_plaquette3<<<(unsigned)e->n_site_tiles, kSiteThreads, kPlaqStageBytes, e->stream>>>(
-        e->d_chains, e->d_site_tiles, e->d_links, e->d_partial);
-    k_chain_reduce_split<<<(unsigned)e->n_chains, 1024, 0, e->stream>>>(
-        e->d_partial, e->d_site_tile_first, tr_partial, ranges, e->d_chains, e->d_result);
+cudaError_t launch_su3_plaquette_from_sweep(ym_ensemble *e, const double *tr_partial) {
+    const SweepLayout &L = e->layouts[e->sweep_layout];
+    if (!L.d_chain_ctas) return cudaErrorInvalidValue;
+    k_chain_reduce_sweep<<<(unsigned)e->n_chains, 1024, 0, e->stream>>>(tr_partial, L.ctas, L.d_chain_ctas,
+                                                                         e->d_chains, e->d_result);
     return cudaGetLastError();
 }
 

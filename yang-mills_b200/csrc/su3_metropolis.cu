@@ -333,9 +333,9 @@ cudaError_t launch_su3_metropolis(ym_ensemble *e, int parity, int mu, double ang
     return tiled_exact::tiled_launch(e, parity, mu, angle, uniform);
 }
 
-cudaError_t launch_su3_metropolis_measure(ym_ensemble *e, double angle, double *tr_partial) {
-    if (e->fast_sweeps) return launch_su3_metropolis_measure_fast(e, angle, tr_partial);
-    return tiled_exact::tiled_launch_measure(e, angle, tr_partial);
+cudaError_t launch_su3_metropolis_measure(ym_ensemble *e, int mu, double angle, double *tr_partial) {
+    if (e->fast_sweeps) return launch_su3_metropolis_measure_fast(e, mu, angle, tr_partial);
+    return tiled_exact::tiled_launch_measure(e, mu, angle, tr_partial);
 }
 
 size_t resident_smem_bytes(const ym_ensemble *e) {

@@ -17,8 +17,8 @@ cudaError_t launch_su3_metropolis_fast(ym_ensemble *e, int parity, int mu, doubl
     return tiled_fast::tiled_launch(e, parity, mu, angle, uniform);
 }
 
-cudaError_t launch_su3_metropolis_measure_fast(ym_ensemble *e, double angle, double *tr_partial) {
-    return tiled_fast::tiled_launch_measure(e, angle, tr_partial);
+cudaError_t launch_su3_metropolis_measure_fast(ym_ensemble *e, int mu, double angle, double *tr_partial) {
+    return tiled_fast::tiled_launch_measure(e, mu, angle, tr_partial);
 }
 
 }  // namespace ym

@@ -727,9 +727,12 @@ __device__ __forceinline__ void term_accumulate(const TermSet &b, m3 &a) {
             }
 }
 
-template <int MU>
+// SAVE = 2 or 4: a_part receives the accumulator after the first SAVE terms
+// (the terms of the first one or two directions other than MU).
+template <int MU, int SAVE = 0>
 __device__ __forceinline__ m3 staple_ring(const double2 *links, const ChainInfo &c, const Coord &x, int par,
-                                          const Nb &pm, const TermSet &s0, const TermSet &s1, int64_t s_self) {
+                                          const Nb &pm, const TermSet &s0, const TermSet &s1, int64_t s_self,
+                                          m3 *a_part = nullptr) {
     constexpr int N0 = Nu<MU, 0>::v, N1 = Nu<MU, 1>::v, N2 = Nu<MU, 2>::v;
     stage_term3<MU, N0>(s0, links, c, term_sites<MU, N0, false>(c, x, par, pm));
     stage_term3<MU, N0>(s1, links, c, term_sites<MU, N0, true>(c, x, par, pm));
@@ -743,12 +746,14 @@ __device__ __forceinline__ m3 staple_ring(const double2 *links, const ChainInfo 
     stage_term3<MU, N1>(s0, links, c, term_sites<MU, N1, false>(c, x, par, pm));
     cp_async_wait_one();
     term_accumulate<true>(s1, a);
+    if (SAVE == 2) *a_part = a;
     stage_term3<MU, N1>(s1, links, c, term_sites<MU, N1, true>(c, x, par, pm));
     cp_async_wait_one();
     term_accumulate<false>(s0, a);
     stage_term3<MU, N2>(s0, links, c, term_sites<MU, N2, false>(c, x, par, pm));
     cp_async_wait_one();
     term_accumulate<true>(s1, a);
+    if (SAVE == 4) *a_part = a;
     stage_term3<MU, N2>(s1, links, c, term_sites<MU, N2, true>(c, x, par, pm));
     cp_async_wait_one();
     term_accumulate<false>(s0, a);
@@ -760,11 +765,15 @@ __device__ __forceinline__ m3 staple_ring(const double2 *links, const ChainInfo 
 
 constexpr int kRingBuffers = 6;   // two sets of three factors
 
-// MEASURE (the last sub-sweep of a sweep, parity 1 and direction 3, with one
-// chain per CTA): each CTA also writes tr_partial[cta] = sum over its links
-// of (1/3) Re Tr(U' A).  Every link in the staple of an odd-site 3-link is
-// final by then, so this is the CTA's share of the plaquettes in planes
-// (0,3), (1,3), (2,3): each such plaquette holds exactly one odd-site 3-link.
+// MEASURE (parity 1, MU = 1, 2 or 3: the last three sub-sweeps of a sweep,
+// one chain per CTA): each CTA also writes tr_partial[cta], the sum over its
+// links of (1/3) Re Tr(U' A_p) with A_p the staple terms of the directions
+// nu < MU (MU = 1: nu = 0; MU = 2: nu = 0, 1; MU = 3: all of A).  Once this
+// sub-sweep has run, every link of those terms is final (directions below
+// MU are done, direction MU's even links were done in parity 0, its odd
+// links here), and each plaquette of plane (nu, MU) holds exactly one
+// odd-site MU-link, so the three launches' sums are the plaquettes of
+// planes (0,1); (0,2), (1,2); (0,3), (1,3), (2,3): all six planes.
 template <int MU, int K, bool MEASURE = false>
 __global__ void __launch_bounds__(T, 2)
 k_su3_metropolis_ring(const ChainInfo *__restrict__ chains, const Tile *__restrict__ tiles,
@@ -786,7 +795,9 @@ k_su3_metropolis_ring(const ChainInfo *__restrict__ chains, const Tile *__restri
         const int64_t s = (int64_t)parity * c.half + t;
         const Coord x = decode_storage(c, s);
         const Nb pm = step(c, x.x, x.lex, parity, MU, +1);
-        const m3 a = staple_ring<MU>(links, c, x, parity, pm, s0, s1, s);
+        constexpr int kSave = (MEASURE && MU == 1) ? 2 : ((MEASURE && MU == 2) ? 4 : 0);
+        m3 a_part;
+        const m3 a = staple_ring<MU, kSave>(links, c, x, parity, pm, s0, s1, s, &a_part);
         cp_async_wait_all();
         m3 u = staged_link(s0.f[0]);
         // the accumulator, for the hits, in the second set's (now free) memory
@@ -796,6 +807,15 @@ k_su3_metropolis_ring(const ChainInfo *__restrict__ chains, const Tile *__restri
         const uint64_t key = link_key(c.seed, sweep, x.lex, MU);
         accepted = visit_ordered<K>(u, sa, c.beta / 3.0, angle, key, tr);
         store_su3(links, c, s, MU, u);
+        if (kSave) {   // Re Tr(U' A_p)
+            double q = 0.0;
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const cplx col[3] = {a_part.e[0][i], a_part.e[1][i], a_part.e[2][i]};
+                q = q + retr_row_fma(u.e[i], col);
+            }
+            tr = q;
+        }
     }
     const unsigned warp_sum = __reduce_add_sync(0xffffffffu, accepted);
     if ((threadIdx.x & 31) == 0 && warp_sum)
@@ -844,11 +864,16 @@ void metro_launch_drawn(ym_ensemble *e, int parity, int mu, double angle, int re
 // its plaquette share (MEASURE): the handle's layout must put one chain in
 // each CTA (128-site items).
 template <int K>
-void metro_launch_measure(ym_ensemble *e, double angle, double *tr_partial) {
+void metro_launch_measure(ym_ensemble *e, int mu, double angle, double *tr_partial) {
     const SweepLayout &L = e->layouts[e->sweep_layout];
-    k_su3_metropolis_ring<3, K, true><<<(unsigned)L.ctas, T, kRingBytes, e->stream>>>(
-        e->d_chains, L.d_items, e->d_links, 1, angle, e->d_sweep, e->d_accepts, L.log2_item,
-        (1 * 4 + 3) & 1, tr_partial);
+    const dim3 g((unsigned)L.ctas), b(T);
+    const int rev = (1 * 4 + mu) & 1;   // the tile order tiled_launch gives (parity 1, mu)
+    if (mu == 1)
+        k_su3_metropolis_ring<1, K, true><<<g, b, kRingBytes, e->stream>>>(e->d_chains, L.d_items, e->d_links, 1, angle, e->d_sweep, e->d_accepts, L.log2_item, rev, tr_partial);
+    else if (mu == 2)
+        k_su3_metropolis_ring<2, K, true><<<g, b, kRingBytes, e->stream>>>(e->d_chains, L.d_items, e->d_links, 1, angle, e->d_sweep, e->d_accepts, L.log2_item, rev, tr_partial);
+    else
+        k_su3_metropolis_ring<3, K, true><<<g, b, kRingBytes, e->stream>>>(e->d_chains, L.d_items, e->d_links, 1, angle, e->d_sweep, e->d_accepts, L.log2_item, rev, tr_partial);
 }
 
 cudaError_t set_smem(const void *f, size_t bytes) {
@@ -867,11 +892,15 @@ cudaError_t configure_kernels() {
     if (configured_device != dev) {
         const void *drawn[4] = {(const void *)k_su3_metropolis<0>, (const void *)k_su3_metropolis<1>,
                                 (const void *)k_su3_metropolis<2>, (const void *)k_su3_metropolis<3>};
-        const void *ordered[10] = {(const void *)k_su3_metropolis_ring<0, 11>, (const void *)k_su3_metropolis_ring<1, 11>,
+        const void *ordered[14] = {(const void *)k_su3_metropolis_ring<0, 11>, (const void *)k_su3_metropolis_ring<1, 11>,
                                    (const void *)k_su3_metropolis_ring<2, 11>, (const void *)k_su3_metropolis_ring<3, 11>,
                                    (const void *)k_su3_metropolis_ring<0, 14>, (const void *)k_su3_metropolis_ring<1, 14>,
                                    (const void *)k_su3_metropolis_ring<2, 14>, (const void *)k_su3_metropolis_ring<3, 14>,
+                                   (const void *)k_su3_metropolis_ring<1, 11, true>,
+                                   (const void *)k_su3_metropolis_ring<2, 11, true>,
                                    (const void *)k_su3_metropolis_ring<3, 11, true>,
+                                   (const void *)k_su3_metropolis_ring<1, 14, true>,
+                                   (const void *)k_su3_metropolis_ring<2, 14, true>,
                                    (const void *)k_su3_metropolis_ring<3, 14, true>};
         for (const void *f : drawn)
             if ((err = set_smem(f, kStageBytes)) != cudaSuccess) return err;
@@ -898,13 +927,13 @@ cudaError_t tiled_launch(ym_ensemble *e, int parity, int mu, double angle, int u
     return cudaGetLastError();
 }
 
-// tiled_launch(e, 1, 3, angle, ordered hits) that also writes each CTA's
-// plaquette share of planes (0,3), (1,3), (2,3) to tr_partial[cta] (the
-// handle's layout must hold one chain per CTA).
-cudaError_t tiled_launch_measure(ym_ensemble *e, double angle, double *tr_partial) {
+// tiled_launch(e, 1, mu, angle, ordered hits), mu = 1, 2 or 3, that also
+// writes each CTA's plaquette share of the planes (nu, mu), nu < mu, to
+// tr_partial[cta] (the handle's layout must hold one chain per CTA).
+cudaError_t tiled_launch_measure(ym_ensemble *e, int mu, double angle, double *tr_partial) {
     if (cudaError_t err = configure_kernels()) return err;
-    if (angle <= 0.3) metro_launch_measure<11>(e, angle, tr_partial);
-    else metro_launch_measure<14>(e, angle, tr_partial);
+    if (angle <= 0.3) metro_launch_measure<11>(e, mu, angle, tr_partial);
+    else metro_launch_measure<14>(e, mu, angle, tr_partial);
     return cudaGetLastError();
 }
 

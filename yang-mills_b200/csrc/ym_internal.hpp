@@ -68,6 +68,7 @@ struct ym_ensemble {
     double *d_result2 = nullptr;
     unsigned long long *d_accepts = nullptr;   // SU(3) accepts / SU(2) heat-bath attempts
     unsigned *d_error = nullptr;               // device error bits (bounded loops that gave up)
+    double *d_tr_partial = nullptr;            // 3 x CTAs: plaquette shares of a measured sweep
     uint64_t *d_sweep = nullptr;           // next sweep index
     uint64_t *d_rng = nullptr;             // reference-replay stream states
     unsigned long long *d_ref_counts = nullptr;  // reference replay: proposals, accepts
@@ -205,15 +206,15 @@ cudaError_t launch_su3_metropolis(ym_ensemble *e, int parity, int mu, double ang
 // The same sub-sweep in the fast form (su3_metropolis_fast.cu);
 // launch_su3_metropolis dispatches to it when e->fast_sweeps is set.
 cudaError_t launch_su3_metropolis_fast(ym_ensemble *e, int parity, int mu, double angle, int uniform);
-// The last sub-sweep of a sweep (parity 1, direction 3, ordered hits), also
-// writing each CTA's share of the plaquettes in planes (0,3), (1,3), (2,3)
-// to tr_partial[cta]; the handle's layout must hold one chain per CTA.
-cudaError_t launch_su3_metropolis_measure(ym_ensemble *e, double angle, double *tr_partial);
-cudaError_t launch_su3_metropolis_measure_fast(ym_ensemble *e, double angle, double *tr_partial);
-// After such a sweep: the plaquettes of planes (0,1), (0,2), (1,2) per site
-// tile, and each chain's average plaquette from both sets of partials
-// (tr_partial and the layout's per-chain CTA ranges) into d_result.
-cudaError_t launch_su3_plaquette_split(ym_ensemble *e, const double *tr_partial);
+// Sub-sweep (parity 1, mu), mu = 1, 2 or 3, with ordered hits, also writing
+// each CTA's share of the plaquettes in planes (nu, mu), nu < mu, to
+// tr_partial[cta]; the handle's layout must hold one chain per CTA.
+cudaError_t launch_su3_metropolis_measure(ym_ensemble *e, int mu, double angle, double *tr_partial);
+cudaError_t launch_su3_metropolis_measure_fast(ym_ensemble *e, int mu, double angle, double *tr_partial);
+// After a sweep whose last three sub-sweeps measured into tr_partial
+// (three arrays of the layout's CTA count): each chain's average plaquette
+// into d_result.
+cudaError_t launch_su3_plaquette_from_sweep(ym_ensemble *e, const double *tr_partial);
 cudaError_t launch_advance_sweep(ym_ensemble *e);
 // Chain-resident sweeps (su3_metropolis.cu): every chain small enough that
 // its links fit in one CTA's shared memory.  series (device, may be null)
