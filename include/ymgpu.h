@@ -118,12 +118,13 @@ int32_t ym_su3_metropolis_sweeps(ym_ensemble *ens, double proposal_angle, int32_
  * graph; series[m * n_chains + chain] receives measurement m.  The sweeps
  * are those of ym_su3_metropolis_sweeps bit for bit.  For binary64 handles
  * with ordered hits whose chains are too large for the chain-resident
- * kernel, the last sub-sweep before each measurement also sums the
- * plaquettes of planes (0,3), (1,3), (2,3) (each link's Re Tr(U'A)) and a
- * three-plane kernel adds the others: the series is then within 1e-12
- * relative of ym_average_plaquette (another summation order); otherwise it
- * is ym_average_plaquette's bit for bit.  ym_su3_measured_run measures the
- * same way. */
+ * kernel, the plaquette comes from the sweep itself: sub-sweeps (parity 1,
+ * direction mu = 1, 2, 3) before each measurement also sum, over their
+ * links, Re Tr(U'A_p) with A_p the staple terms of the directions below mu,
+ * which are exactly the plaquettes of the planes (nu, mu), nu < mu.  The
+ * series is then within 1e-12 relative of ym_average_plaquette (another
+ * summation order); otherwise it is ym_average_plaquette's bit for bit.
+ * ym_su3_measured_run measures the same way. */
 int32_t ym_su3_measured_sweeps(ym_ensemble *ens, double proposal_angle, int32_t generator_mode,
                                int64_t n_measurements, int64_t sweeps_per_measurement,
                                double *series);

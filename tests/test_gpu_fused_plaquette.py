@@ -2,10 +2,11 @@
 ym_su3_measured_run).
 
 For binary64 handles with ordered hits whose chains are too large for the
-chain-resident kernel, the last sub-sweep of each measured sweep (parity 1,
-direction 3) sums (1/3) Re Tr(U' A) of its links, which are the plaquettes
-of planes (0,3), (1,3), (2,3), and a three-plane kernel adds the others.
-The sweeps themselves are unchanged, so:
+chain-resident kernel, sub-sweeps (parity 1, direction mu = 1, 2, 3) of each
+measured sweep sum (1/3) Re Tr(U' A_p) of their links, A_p the staple terms
+of the directions below mu: the plaquettes of planes (0,1); (0,2), (1,2);
+(0,3), (1,3), (2,3).  No plaquette kernel runs.  The sweeps themselves are
+unchanged, so:
 
   * the links, accept counts and sweep index after measured sweeps are
     bitwise those of the same sweeps launched directly;
