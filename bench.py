@@ -761,7 +761,7 @@ def main():
             "plaquette_mean": float(np.mean(plaq)),
             "acceptance": leg["acceptance"],
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-            "gpu_launches": int(args.steps * 12),   # 8 sub-sweeps, sweep counter, plaquette, reduction, series store
+            "gpu_launches": int(args.steps * 11),   # 8 sub-sweeps (3 measuring), sweep counter, reduction, series store
             "clocks": leg["clocks"],
             "clocks_leg": dict(leg["clocks_leg"] or {}, note="every sample of the FP64 leg: "
                                "warm-up, timed steps and the sampler's start and stop"),
