@@ -282,28 +282,41 @@ def main():
         timed with CUDA events on the handle's stream.  measured(n) runs n
         steps through the library's measured-sweeps entry point (one captured
         graph per step, the plaquette of every step stored on the device and
-        read back once at the end) and returns the plaquette series.  A second
-        pass of the same steps issued one launch at a time with event pairs
-        around each launch (step() = one sweep, then average_plaquette) gives
-        the dominant kernel's per-launch time and its share of a step.  With
-        sampler_clocks, nvidia-smi samples every 10 ms from before the warm-up
-        to after the timed steps: "clocks" summarises the samples inside the
-        timed region, "clocks_leg" all of them."""
+        read back once) and returns the plaquette series.  The last n_prof
+        steps of the timed region are issued one launch at a time with an
+        event pair around each launch (step() = one sweep, then
+        average_plaquette): they give the dominant kernel's per-launch time
+        and its share of a step, inside the timed region.  With
+        sampler_clocks, nvidia-smi samples every 10 ms from before the
+        warm-up to after the timed steps: "clocks" summarises the samples
+        inside the timed region, "clocks_leg" all of them."""
         sampler = ClockSampler(local) if sampler_clocks else None
         if sampler:
             sampler.__enter__()
             sampler.wait_first()
         measured(args.warmup)
+        step()
+        ens.average_plaquette()
         ens.synchronize()
+        n_prof = max(1, min(20, args.steps // 4))
+        n_graph = args.steps - n_prof
         stream = torch.cuda.ExternalStream(ens.stream(), device=local)
         start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        pa, pb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         p0, a0 = ens.accounting()
         barrier()
         torch.cuda.synchronize()
         if sampler:
             sampler.wait_first()
         start.record(stream)
-        series = measured(args.steps)
+        series = measured(n_graph) if n_graph > 0 else np.zeros((0, 1))
+        plaq = [float(v) for v in np.asarray(series)[:, 0]]
+        ens.profile(True)
+        pa.record(stream)
+        for _ in range(n_prof):
+            step()
+            plaq.append(float(ens.average_plaquette()[0]))
+        pb.record(stream)
         stop.record(stream)
         stop.synchronize()
         torch.cuda.synchronize()
@@ -312,20 +325,9 @@ def main():
             sampler.__exit__(None, None, None)
         barrier()
         ms = max_over_ranks(start.elapsed_time(stop))
-        p1, a1 = ens.accounting()
-        plaq = [float(v) for v in np.asarray(series)[:, 0]]
-        # per-launch pass
-        n_prof = max(3, min(args.steps, 20))
-        ens.profile(True)
-        pa, pb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        pa.record(stream)
-        for _ in range(n_prof):
-            step()
-            ens.average_plaquette()
-        pb.record(stream)
-        pb.synchronize()
         k_ms, k_launches = ens.profile_read(kernel)
         ens.profile(False)
+        p1, a1 = ens.accounting()
         launch_s = k_ms * 1e-3 / max(1, k_launches)
         bytes_per_launch = (volume // 2) * LINKS_PER_UPDATE * link_bytes
         achieved = bytes_per_launch / launch_s / 1e9
@@ -337,7 +339,9 @@ def main():
                          "launch_ms": launch_s * 1e3,
                          "kernel_share_of_step": k_ms / max(1e-9, pa.elapsed_time(pb)),
                          "bytes_per_launch": bytes_per_launch,
-                         "per_launch_pass_steps": n_prof},
+                         "per_launch_steps": n_prof,
+                         "note": f"per-launch events over the last {n_prof} of the {args.steps} timed steps, "
+                                 "issued launch by launch (the others through the measured-sweeps graphs)"},
             "clocks": sampler.summary() if sampler else None,
             "clocks_leg": sampler.summary(whole=True) if sampler else None,
         }
@@ -761,7 +765,10 @@ def main():
             "plaquette_mean": float(np.mean(plaq)),
             "acceptance": leg["acceptance"],
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-            "gpu_launches": int(args.steps * 11),   # 8 sub-sweeps (3 measuring), sweep counter, reduction, series store
+            # measured steps: 8 sub-sweeps (3 measuring), sweep counter, reduction, series store;
+            # per-launch steps: 8 sub-sweeps, sweep counter, plaquette, reduction
+            "gpu_launches": int((args.steps - leg["roofline"]["per_launch_steps"]) * 11
+                                + leg["roofline"]["per_launch_steps"] * 11),
             "clocks": leg["clocks"],
             "clocks_leg": dict(leg["clocks_leg"] or {}, note="every sample of the FP64 leg: "
                                "warm-up, timed steps and the sampler's start and stop"),
